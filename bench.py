@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Benchmark: HISQ multishift CG to a per-shift true relative residual of 1e-10 on one B200 per rank.
+
+Workload (one step = one complete multishift solve of one system):
+  32^4 lattice, thin links U = exp(i*0.3*H) (seeded Gaussian traceless Hermitian H), staggered phases folded in,
+  fat = 9/8 U, long = -1/24 U U U, mass m = 0.05, 12 shifts sigma_i log-spaced 1e-4..1 (absolute shifts
+  m^2 + sigma_i), Gaussian even-site source.  Synthetic data generated on the device from a seed.
+
+  value : solves/s over all ranks, inputs resident in HBM (kq_solve_multishift_device)
+  e2e   : the same through the reference-facing call kuqcd_solve_multishift with host (pinned) buffers,
+          host<->device copies inside the timed region
+  roofline : the dominant kernel (the dslash of the solver's precision), algorithmic bytes / CUDA-event time
+  cpu_baseline : the reference's own CPU solver (oracle/_ref, all host cores) on a bounded sample of the solve
+
+`--impl reference` times the reference CPU implementation alone (rank 0) and prints its own JSON line.
+Multi-GPU: every rank solves an independent system (different seed): weak scaling, no data-path collective.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "HISQ dslash GFLOP/s + HBM GB/s; multishift CG time to 1e-10, mixed vs plain FP64"
+DIMS = (32, 32, 32, 32)
+EPS, MASS, NSHIFT = 0.3, 0.05, 12
+REL_RES = 1e-10
+DSLASH_FLOPS = 1146          # per output site
+DSLASH_BYTES = {8: 2400, 4: 1200, 2: 608}   # compulsory bytes per output site: 16 links + 1 in + 1 out spinor
+# Iterations the reference CGM (inverter_cgm.cpp:17-87) needs on this workload (seed 1000, tol (1e-10)^2 |b|^2,
+# reference-semantics shifts), measured by running oracle/ref_iterations.py to convergence.
+REF_ITERS_32 = None
+
+
+def shifts_abs():
+    return list(MASS * MASS + np.logspace(-4, 0, NSHIFT))
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import kuqcd_b200 as K
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=600))
+    dims = tuple(args.dims)
+    V = int(np.prod(dims))
+    Vh = V // 2
+    seed = 1000 + rank
+    ctx = K.Context(dims, device=local)
+    dfat = torch.empty(V * 72, dtype=torch.float64, device="cuda")
+    dlng = torch.empty(V * 72, dtype=torch.float64, device="cuda")
+    ctx.make_links(EPS, seed, dfat, dlng)
+    hfat, hlng = dfat.cpu().numpy(), dlng.cpu().numpy()
+    del dfat, dlng
+    ctx.load_links(K.KUQCD_FAT_LINK, hfat)
+    ctx.load_links(K.KUQCD_LONG_LINK, hlng)
+    db = torch.empty(Vh * 6, dtype=torch.float64, device="cuda")
+    ctx.make_source(0, seed, db)
+    vb = ctx.spinor_bytes(K.KUQCD_DOUBLE)
+    d_b = torch.empty(vb, dtype=torch.uint8, device="cuda")
+    ctx.upload(K.KUQCD_DOUBLE, db.cpu().numpy(), d_b)
+    d_x = torch.empty(vb * NSHIFT, dtype=torch.uint8, device="cuda")
+    sig = shifts_abs()
+    hb = db.cpu().numpy()
+    bnorm2 = float(hb @ hb)
+
+    solver = K.KQ_SOLVER_MIXED if args.solver == "mixed" else K.KQ_SOLVER_CGM
+    sprec = {"mixed": K.KUQCD_SINGLE, "fp64": K.KUQCD_DOUBLE}[args.solver]
+    # plain CGM stopping rule tol = (rel * |b|)^2 on the recursive residual of every shift
+    kw = dict(parity=0, solver=solver, prec=sprec, max_iter=100000, tol=(REL_RES ** 2) * bnorm2,
+              rel_residual=REL_RES, shift_mode=1)
+
+    def step_device():
+        return ctx.solve_device(d_b, d_x, sig, **kw)
+
+    for _ in range(args.warmup):
+        info = step_device()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    iters = []
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            info = step_device()
+            iters.append(info.iter)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    # the library's own stream is synchronised at the end of every solve; the events bracket the whole loop
+    ms_step = ms / args.steps
+    true_res = ctx.true_residuals(0, sig, d_b, d_x)
+    if world > 1:
+        t = torch.tensor([ms_step], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+        dist.barrier()
+
+    # ---------------- e2e: reference-facing call with pinned host buffers
+    hb_pin = torch.from_numpy(hb).pin_memory()
+    hx_pin = [torch.empty(Vh * 6, dtype=torch.float64).pin_memory() for _ in range(NSHIFT)]
+    os.environ["KUQCD_SOLVER"] = "mixed" if args.solver == "mixed" else "fp64"
+    K.kuqcd_gauge_free()
+    K.kuqcd_init()
+    gp = K.KuQCDGaugeParam()
+    gp.lat[:] = dims
+    gp.halo_depth, gp.od, gp.site_subset = 0, K.KUQCD_TZYX_ORDER, K.KUQCD_ALL
+    gp.gauge_order, gp.prec, gp.recon = K.KUQCD_NORMAL_ORDER, K.KUQCD_DOUBLE, K.KUQCD_GAUGE_RECON_NO
+    gp.link_type = K.KUQCD_FAT_LINK
+    assert K.kuqcd_load_gaugefield(hfat, gp) == 0
+    gp.link_type = K.KUQCD_LONG_LINK
+    assert K.kuqcd_load_gaugefield(hlng, gp) == 0
+    refsh = [sig[0]] + [s - sig[0] for s in sig[1:]]
+    shc = (C.c_double * NSHIFT)(*refsh)
+    ip = K.KuQCDInvertParam(dslash_type=K.KUQCD_HISQPC_DIRAC, inverter_type=K.KUQCD_CGM,
+                            matpc_type=K.KUQCD_EVEN_EVEN, prec=K.KUQCD_DOUBLE, num_shift=NSHIFT, max_iter=100000,
+                            iter=0, tol=(REL_RES ** 2) * bnorm2, shifts=C.cast(shc, C.POINTER(C.c_double)))
+    xs_np = [x.numpy() for x in hx_pin]
+    b_np = hb_pin.numpy()
+    for _ in range(max(1, args.warmup)):
+        assert K.kuqcd_solve_multishift(xs_np, b_np, ip) == 0
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        assert K.kuqcd_solve_multishift(xs_np, b_np, ip) == 0
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    K.kuqcd_gauge_free()
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    # ---------------- dslash roofline: the solver's dominant kernel, CUDA events on the launching stream
+    dsl = {}
+    for name, prec in [("fp64", K.KUQCD_DOUBLE), ("fp32", K.KUQCD_SINGLE), ("half", K.KUQCD_HALF)]:
+        nbp = ctx.spinor_bytes(prec)
+        a = torch.zeros(nbp, dtype=torch.uint8, device="cuda")
+        o = torch.zeros(nbp, dtype=torch.uint8, device="cuda")
+        ctx.convert(d_b, K.KUQCD_DOUBLE, a, prec, stream.cuda_stream)
+        for _ in range(3):
+            ctx.dslash(prec, a, o, 1, stream.cuda_stream)
+        reps = 20
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for r in range(reps):
+            ctx.dslash(prec, a if r % 2 == 0 else o, o if r % 2 == 0 else a, 1 - (r % 2), stream.cuda_stream)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        t_launch = s0.elapsed_time(s1) / reps * 1e-3
+        dsl[name] = {"ms": t_launch * 1e3, "gflops": DSLASH_FLOPS * Vh / t_launch / 1e9,
+                     "gbs": DSLASH_BYTES[prec] * Vh / t_launch / 1e9}
+    dom = "fp64" if args.solver == "fp64" else "fp32"
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs")
+    peak_note = "measured" if peak else "fallback"
+    peak = peak or 6650.0
+    achieved = dsl[dom]["gbs"]
+
+    result = None
+    if rank == 0:
+        cpu = cpu_baseline_sample(args) if (world == 1 and not args.no_cpu_baseline) else None
+        kernels_per_iter = 4
+        launches = sum(1 + kernels_per_iter * 8 * ((it + 7) // 8) for it in iters)
+        result = {
+            "metric": METRIC,
+            "value": world * 1000.0 / ms_step,
+            "unit": "solves/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64" if args.solver == "fp64" else "f32+f64",
+            "data": "synthetic (seeded on device: exp(i eps H) thin links, Gaussian source)",
+            "config": {"workload": f"multishift CG {'x'.join(map(str, dims))}, {NSHIFT} shifts 1e-4..1, m={MASS}, "
+                                   f"eps={EPS}, per-shift true residual {REL_RES}",
+                       "solver": args.solver, "lattice": list(dims), "shifts": NSHIFT,
+                       "iterations": iters[-1], "max_true_residual": max(true_res),
+                       "l2": "inputs larger than L2 (links 1.2 GB FP64)", "parallelism": f"replicas x{world}"},
+            "e2e": {"value": world / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": Vh * 6 * 8,
+                    "d2h_bytes_per_step": NSHIFT * Vh * 6 * 8},
+            "roofline": {"bound": "hbm", "kernel": f"dslash_kernel<{dom}>", "achieved": achieved, "peak": peak,
+                         "peak_source": peak_note, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "bytes_per_site": DSLASH_BYTES[8 if dom == 'fp64' else 4]},
+            "dslash": dsl,
+            "cpu_baseline": cpu,
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(result))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    ctx.close()
+    return result
+
+
+# ---------------------------------------------------------------------------------------------- CPU reference
+def ref_iterations_needed():
+    return REF_ITERS_32
+
+
+def ref_cpu_time_per_iter(dims, sample_iters, seed=1000):
+    """Time `sample_iters` iterations of the reference CGM (oracle/_ref, all host cores) on the bench workload."""
+    from oracle import oracle as O
+
+    fat, lng = O.make_links(dims, EPS, seed)
+    b = O.make_source(dims, 0, seed)
+    sig = shifts_abs()
+    refsh = [sig[0]] + [s - sig[0] for s in sig[1:]]
+    tol = (REL_RES ** 2) * float(b @ b)
+    t0 = time.perf_counter()
+    st, xs, it = O.ref_solve(dims, fat, lng, b, refsh, tol, sample_iters)
+    t1 = time.perf_counter()
+    assert st == 0 and it == sample_iters
+    return (t1 - t0) / sample_iters
+
+
+def cpu_baseline_sample(args):
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        return None
+    dims = tuple(args.dims)
+    sample = args.cpu_sample_iters
+    t_it = ref_cpu_time_per_iter(dims, sample)
+    iters = ref_iterations_needed() or 0
+    solve_s = t_it * iters if iters else None
+    return {"value": (1.0 / solve_s) if solve_s else None, "unit": "solves/s", "cores": os.cpu_count(),
+            "kind": "reference", "seconds_per_iteration": t_it,
+            "sample": f"{sample} CGM iterations of the reference on the same workload, extrapolated to "
+                      f"{iters} iterations (its iteration count to convergence)"}
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return None
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libkuqcd_ref.so was not built"}))
+        return None
+    dims = tuple(args.dims)
+    sample = args.cpu_sample_iters
+    for _ in range(args.warmup):
+        ref_cpu_time_per_iter(dims, max(1, sample // 4))
+    times = [ref_cpu_time_per_iter(dims, sample) for _ in range(args.steps)]
+    t_it = float(np.mean(times))
+    iters = ref_iterations_needed()
+    solve_s = t_it * iters
+    v = 1.0 / solve_s
+    res = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": solve_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": f"multishift CG {'x'.join(map(str, dims))}, {NSHIFT} shifts 1e-4..1, m={MASS}, "
+                               f"eps={EPS}, per-shift true residual {REL_RES}", "solver": "reference CGM (CPU)"},
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": os.cpu_count(), "kind": "reference",
+                         "sample": f"{sample} CGM iterations per step, extrapolated to {iters} iterations"},
+        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(res))
+    return res
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--solver", choices=["mixed", "fp64"], default="fp64")
+    ap.add_argument("--dims", type=int, nargs=4, default=list(DIMS))
+    ap.add_argument("--cpu-sample-iters", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

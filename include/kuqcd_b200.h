@@ -1,0 +1,126 @@
+/*
+ * kuqcd_b200 — C ABI of the B200 (sm_100a) HISQ dslash + multishift CG library (libkuqcd_b200.so).
+ *
+ * Plain pointers and sizes only.  Precision arguments use KuQCDPrecision values (DOUBLE = 8, SINGLE = 4,
+ * HALF = 2).  `stream` arguments are cudaStream_t values passed as void*; NULL selects the context's own stream.
+ * Every call returns a KuQCDStatus (0 = success); kq_last_error() gives the message of the last failure on the
+ * calling thread.
+ *
+ * Host record layouts are the reference's NORMAL_ORDER layouts (kuqcd.cpp:103-169):
+ *   gauge  h[reim + 2*(l + 9*(dir + 4*s))], s in [0,V): even sites first, then odd; l = col + 3*row
+ *   spinor h[reim + 2*(c + 3*i_cb)] over one parity, i_cb = (x>>1) + (nx/2)*(y + ny*(z + nz*t))
+ * BATCH_ORDER gauge records (kuqcd.cpp:112-124) are accepted by the kuqcd API twins below.
+ */
+#ifndef KUQCD_B200_H
+#define KUQCD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "kuqcd_enum.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ================================================================ reference-facing entry points
+ * C-linkage twins of the five exported calls of include/kuqcd.h:29-34 (the C++ kuqcd:: versions in kuqcd.h
+ * forward to these).  Same arguments, same status codes, same call order and ownership rules. */
+
+/* replaces kuqcd::kuqcd_init (kuqcd.cpp:288-301) */
+KuQCDStatus kq_kuqcd_init(void);
+/* replaces kuqcd::kuqcd_load_gaugefield (kuqcd.cpp:303-402) */
+KuQCDStatus kq_kuqcd_load_gaugefield(void *h_gauge, KuQCDGaugeParam *param);
+/* replaces kuqcd::kuqcd_solve_multishift (kuqcd.cpp:404-445) */
+KuQCDStatus kq_kuqcd_solve_multishift(void **hp_x, void *hp_b, KuQCDInvertParam *param);
+/* replaces kuqcd::kuqcd_gauge_free (kuqcd.cpp:447-476) */
+void kq_kuqcd_gauge_free(void);
+/* replaces kuqcd::kuqcd_end (kuqcd.cpp:477-487) */
+void kq_kuqcd_end(void);
+
+/* ================================================================ device-level API
+ * A context owns one lattice on one GPU: the device-resident links (FP64 master plus FP32 / HALF copies made on
+ * demand), a stream and the solver workspaces.  It replaces the reference's LattBase + GaugeField pair
+ * (latt_base.h:19-50, gauge_field.h:19-45) for one rank. */
+typedef struct kq_context kq_context;
+
+/* lat = {nx, ny, nz, nt}; nx must be even (checkerboarding, latt_base.cpp:114-116). */
+KuQCDStatus kq_context_create(const unsigned lat[4], int device, kq_context **out);
+void kq_context_destroy(kq_context *ctx);
+
+/* Copy one link field (KUQCD_FAT_LINK or KUQCD_LONG_LINK) from a NORMAL_ORDER host record of precision
+ * host_prec to the device.  Replaces kuqcd_gaugefield_set_values (kuqcd.cpp:103-127). */
+KuQCDStatus kq_load_links(kq_context *ctx, int link_type, const void *host, int host_prec);
+/* Make both link fields resident in precision prec (SINGLE or HALF copies derived from the loaded master). */
+KuQCDStatus kq_prepare_links(kq_context *ctx, int prec);
+
+/* Bytes of one parity spinor field in the device layout of precision prec. */
+size_t kq_spinor_bytes(const kq_context *ctx, int prec);
+/* Host record (precision host_prec) <-> device field (precision prec).  Replaces kuqcd_spinorfield_set/get_values
+ * (kuqcd.cpp:129-169). */
+KuQCDStatus kq_spinor_upload(kq_context *ctx, int prec, const void *host, int host_prec, void *d_field, void *stream);
+KuQCDStatus kq_spinor_download(kq_context *ctx, int prec, const void *d_field, void *host, int host_prec,
+                               void *stream);
+/* Precision conversion between two device fields of the same parity. */
+KuQCDStatus kq_spinor_convert(kq_context *ctx, const void *d_src, int src_prec, void *d_dst, int dst_prec,
+                              void *stream);
+
+/* d_dst (parity dst_parity) = D d_src (other parity).  Replaces DiracHISQ::Dslash (dirac_hisq.cpp:409-455). */
+KuQCDStatus kq_dslash(kq_context *ctx, int prec, const void *d_src, void *d_dst, int dst_parity, void *stream);
+/* d_dst = sigma*d_src - D_pq D_qp d_src on parity `parity`; d_tmp holds one field of the other parity.
+ * Replaces DiracHISQ::MdaggM (dirac_hisq.cpp:457-462) followed by Axmy (spinor_field.cpp:130-144). */
+KuQCDStatus kq_mdagm(kq_context *ctx, int prec, double sigma, const void *d_src, void *d_dst, void *d_tmp,
+                     int parity, void *stream);
+
+/* ---------------------------------------------------------------- solver */
+enum {
+    KQ_SOLVER_CGM = 0,        /* multishift CG with the reference's recurrences (CGM::Invert), FP64 or FP32 */
+    KQ_SOLVER_MIXED = 1       /* sloppy multishift + per-shift reliable-update refinement to an FP64 target */
+};
+
+typedef struct {
+    int parity;               /* 0: source and solutions on even sites (EVEN_EVEN), 1: odd (ODD_ODD) */
+    int num_shift;            /* 1..64 */
+    const double *shifts;     /* see shift_mode */
+    int shift_mode;           /* 0: reference semantics, x_j solves (shifts[0] + shifts[j] - DD) for j >= 1
+                                 1: absolute, x_j solves (shifts[j] - DD) x = b */
+    int solver;               /* KQ_SOLVER_* */
+    int prec;                 /* KQ_SOLVER_CGM: DOUBLE or SINGLE; KQ_SOLVER_MIXED: sloppy SINGLE or HALF */
+    int host_prec;            /* precision of the host b / x records */
+    int max_iter;
+    double tol;               /* KQ_SOLVER_CGM: reference stopping rule zeta_k^2 |r|^2 < tol */
+    double rel_residual;      /* KQ_SOLVER_MIXED: per-shift true relative residual target */
+} kq_solve_param;
+
+typedef struct {
+    int iter;                 /* multishift iterations */
+    int iter_refine;          /* refinement iterations summed over shifts (KQ_SOLVER_MIXED) */
+    int status;               /* 0 ok, 1 breakdown, 2 max_iter reached */
+    int num_shift;
+    double true_residual[64]; /* |b - (sigma_k - DD) x_k| / |b| in FP64, when computed */
+    double seconds;           /* device time of the solve */
+} kq_solve_info;
+
+/* Host b (num Vh*6 values of host_prec) -> host x[k].  Copies in, solves on the device, copies out. */
+KuQCDStatus kq_solve_multishift(kq_context *ctx, const kq_solve_param *param, const void *host_b,
+                                void *const *host_x, kq_solve_info *info);
+/* Same with device fields in FP64 (d_b: one field; d_x: num_shift fields, kq_spinor_bytes(ctx, 8) apart). */
+KuQCDStatus kq_solve_multishift_device(kq_context *ctx, const kq_solve_param *param, const void *d_b, void *d_x,
+                                       kq_solve_info *info);
+/* FP64 true relative residuals |b - (sigma_k - DD) x_k| / |b| of device FP64 fields (absolute sigmas). */
+KuQCDStatus kq_true_residuals(kq_context *ctx, int parity, int num_shift, const double *sigma, const void *d_b,
+                              const void *d_x, double *out);
+
+/* ---------------------------------------------------------------- synthetic fields
+ * thin U = exp(i eps H), H traceless Hermitian from seeded Gaussians; staggered phases folded in;
+ * fat = 9/8 U, long = -1/24 U(x) U(x+mu) U(x+2mu); written as FP64 NORMAL_ORDER host records into DEVICE
+ * buffers of V*72 doubles each.  Source: Gaussian colour vectors on one parity (Vh*6 doubles). */
+KuQCDStatus kq_make_links_record(kq_context *ctx, double eps, uint64_t seed, double *d_fat, double *d_long);
+KuQCDStatus kq_make_source_record(kq_context *ctx, int parity, uint64_t seed, double *d_b);
+
+const char *kq_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,525 @@
+// C ABI of libkuqcd_b200.so: contexts, link loading, dslash, solver entry points and the C-linkage twins of the
+// reference's five exported calls (kuqcd.cpp:288-487).
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "kq_internal.h"
+#include "kq_prec.cuh"
+#include "kq_solver.h"
+
+namespace kq {
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+const char *last_error() { return g_last_error.c_str(); }
+
+cudaError_t launch_mdagm(const Geom &g, const GaugeDev &gd, int prec, double sigma, const void *src, void *tmp,
+                         void *dst, int parity, cudaStream_t s);
+cudaError_t mixed_solve(struct ::kq_context *ctx, const kq_solve_param *param, const double *shifts_abs,
+                        const void *d_b, void *d_x, kq_solve_info *info);
+cudaError_t true_residuals(const Geom &g, const GaugeDev &gd, int parity, int ns, const double *sigma,
+                           const void *d_b, const void *d_x, size_t xstride, void *d_tmp, void *d_s, double *partials,
+                           double *out, cudaStream_t s);
+
+}  // namespace kq
+
+using namespace kq;
+
+// ------------------------------------------------------------------------------------------------ context
+struct kq_context {
+    int device = 0;
+    unsigned lat[4] = {0, 0, 0, 0};
+    Geom g{};
+    cudaStream_t stream = nullptr;
+    GaugeDev gd;
+    int master = -1;  // precision of the loaded links (P64 or P32)
+    bool fat_loaded = false, long_loaded = false;
+    unsigned *d_scratch = nullptr;
+    // solver workspace (grown on demand)
+    void *work = nullptr;
+    size_t work_bytes = 0;
+    CgmPoll *poll = nullptr;  // pinned
+};
+
+namespace kq {
+
+// Workspace carving helper: 256-byte aligned bump allocator over ctx->work.
+struct Carve {
+    char *base;
+    size_t off = 0;
+    explicit Carve(void *b) : base(static_cast<char *>(b)) {}
+    void *take(size_t n)
+    {
+        off = (off + 255) & ~size_t(255);
+        void *p = base ? base + off : nullptr;
+        off += n;
+        return p;
+    }
+};
+
+cudaError_t ensure_work(::kq_context *ctx, size_t bytes)
+{
+    if (ctx->work_bytes >= bytes) return cudaSuccess;
+    if (ctx->work) {
+        KQ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        cudaFree(ctx->work);
+        ctx->work = nullptr;
+        ctx->work_bytes = 0;
+    }
+    KQ_CUDA_TRY(cudaMalloc(&ctx->work, bytes));
+    ctx->work_bytes = bytes;
+    return cudaSuccess;
+}
+
+static cudaError_t alloc_links(::kq_context *ctx, int prec)
+{
+    if (ctx->gd.block[prec]) return cudaSuccess;
+    const size_t lb = links_bytes(ctx->g, prec);
+    void *blk = nullptr;
+    KQ_CUDA_TRY(cudaMalloc(&blk, 4 * lb));
+    ctx->gd.block[prec] = blk;
+    char *b = static_cast<char *>(blk);
+    ctx->gd.fat[prec].par[0] = b;
+    ctx->gd.fat[prec].par[1] = b + lb;
+    ctx->gd.lng[prec].par[0] = b + 2 * lb;
+    ctx->gd.lng[prec].par[1] = b + 3 * lb;
+    ctx->gd.fat[prec].scale = ctx->gd.lng[prec].scale = 1.f;
+    return cudaSuccess;
+}
+
+static void free_links(::kq_context *ctx, int prec)
+{
+    if (ctx->gd.block[prec]) cudaFree(ctx->gd.block[prec]);
+    ctx->gd.block[prec] = nullptr;
+    ctx->gd.have[prec] = false;
+}
+
+KuQCDStatus status_of(cudaError_t e)
+{
+    if (e == cudaSuccess) return KUQCD_SUCCESS;
+    if (e == cudaErrorMemoryAllocation) return KUQCD_ERR_NO_MEMORY;
+    if (e == cudaErrorInvalidValue) return KUQCD_ERR_INVALID_PARAM;
+    return KUQCD_ERR_UNKNOWN_ERROR;
+}
+
+}  // namespace kq
+
+#define KQ_API extern "C" __attribute__((visibility("default")))
+
+static cudaStream_t pick_stream(kq_context *ctx, void *stream)
+{
+    return stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+}
+
+KQ_API const char *kq_last_error(void) { return kq::last_error(); }
+
+KQ_API KuQCDStatus kq_context_create(const unsigned lat[4], int device, kq_context **out)
+{
+    if (!lat || !out) {
+        set_last_error("kq_context_create: null pointer");
+        return KUQCD_ERR_NULL_POINTER;
+    }
+    for (int i = 0; i < 4; ++i)
+        if (lat[i] == 0) {
+            set_last_error("kq_context_create: lattice extent is 0");
+            return KUQCD_ERR_INVALID_PARAM;
+        }
+    if (lat[0] & 1u) {
+        set_last_error("kq_context_create: x extent must be even for even-odd preconditioning");
+        return KUQCD_ERR_INVALID_PARAM;
+    }
+    const double V = (double)lat[0] * lat[1] * lat[2] * lat[3];
+    if (V / 2 > 2.0e9) {
+        set_last_error("kq_context_create: more than 2^31 sites per parity");
+        return KUQCD_ERR_INVALID_PARAM;
+    }
+    kq_context *c = new (std::nothrow) kq_context();
+    if (!c) return KUQCD_ERR_NO_MEMORY;
+    c->device = device;
+    memcpy(c->lat, lat, sizeof(c->lat));
+    c->g = make_geom(lat);
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_scratch, 256);
+    if (e == cudaSuccess) e = cudaMallocHost(&c->poll, 4096);
+    if (e != cudaSuccess) {
+        set_last_error(std::string("kq_context_create: ") + cudaGetErrorString(e));
+        if (c->stream) cudaStreamDestroy(c->stream);
+        if (c->d_scratch) cudaFree(c->d_scratch);
+        delete c;
+        return status_of(e);
+    }
+    *out = c;
+    return KUQCD_SUCCESS;
+}
+
+KQ_API void kq_context_destroy(kq_context *ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (int p = 0; p < 3; ++p) free_links(ctx, p);
+    if (ctx->work) cudaFree(ctx->work);
+    if (ctx->d_scratch) cudaFree(ctx->d_scratch);
+    if (ctx->poll) cudaFreeHost(ctx->poll);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+KQ_API KuQCDStatus kq_load_links(kq_context *ctx, int link_type, const void *host, int host_prec)
+{
+    if (!ctx || !host) {
+        set_last_error("kq_load_links: null pointer");
+        return KUQCD_ERR_NULL_POINTER;
+    }
+    if (link_type != KUQCD_FAT_LINK && link_type != KUQCD_LONG_LINK) {
+        set_last_error("kq_load_links: link_type is invalid");
+        return KUQCD_ERR_INVALID_PARAM;
+    }
+    const int rp = prec_from_api(host_prec);
+    if (rp != P64 && rp != P32) {
+        set_last_error("kq_load_links: host precision must be DOUBLE or SINGLE");
+        return host_prec == KUQCD_HALF ? KUQCD_ERR_UNSUPPORTED : KUQCD_ERR_INVALID_PARAM;
+    }
+    cudaSetDevice(ctx->device);
+    if (ctx->master < 0) ctx->master = rp;
+    const int mp = ctx->master;
+    cudaError_t e = alloc_links(ctx, mp);
+    if (e != cudaSuccess) return status_of(e);
+    const size_t V = 2 * (size_t)ctx->g.vh;
+    const size_t rec_bytes = V * 72 * (rp == P64 ? 8 : 4);
+    void *stage = nullptr;
+    e = cudaMalloc(&stage, rec_bytes);
+    if (e != cudaSuccess) {
+        set_last_error("kq_load_links: cannot stage the host record on the device");
+        return status_of(e);
+    }
+    e = cudaMemcpyAsync(stage, host, rec_bytes, cudaMemcpyHostToDevice, ctx->stream);
+    // fold the reference kernel's factors into the device links: 1/2 for fat, c3 = -1/48 for long
+    const double factor = link_type == KUQCD_FAT_LINK ? 0.5 : -1.0 / 48.0;
+    LinkSet &dst = link_type == KUQCD_FAT_LINK ? ctx->gd.fat[mp] : ctx->gd.lng[mp];
+    if (e == cudaSuccess) e = links_from_host_record(ctx->g, stage, rp, factor, dst, mp, ctx->d_scratch, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(stage);
+    if (e != cudaSuccess) {
+        set_last_error(std::string("kq_load_links: ") + cudaGetErrorString(e));
+        return status_of(e);
+    }
+    if (link_type == KUQCD_FAT_LINK) ctx->fat_loaded = true;
+    else ctx->long_loaded = true;
+    ctx->gd.have[mp] = ctx->fat_loaded && ctx->long_loaded;
+    // derived copies are stale now
+    for (int p = 0; p < 3; ++p)
+        if (p != mp) free_links(ctx, p);
+    return KUQCD_SUCCESS;
+}
+
+KQ_API KuQCDStatus kq_prepare_links(kq_context *ctx, int prec)
+{
+    if (!ctx) return KUQCD_ERR_NULL_POINTER;
+    const int p = prec_from_api(prec);
+    if (p < 0) {
+        set_last_error("kq_prepare_links: invalid precision");
+        return KUQCD_ERR_INVALID_PARAM;
+    }
+    if (!ctx->fat_loaded || !ctx->long_loaded) {
+        set_last_error("kq_prepare_links: load the fat and long links first");
+        return KUQCD_ERR_UNEXPECTED_CALL_ORDER;
+    }
+    if (ctx->gd.have[p]) return KUQCD_SUCCESS;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = alloc_links(ctx, p);
+    if (e == cudaSuccess)
+        e = links_convert(ctx->g, ctx->gd.fat[ctx->master], ctx->master, ctx->gd.fat[p], p, ctx->d_scratch, ctx->stream);
+    if (e == cudaSuccess)
+        e = links_convert(ctx->g, ctx->gd.lng[ctx->master], ctx->master, ctx->gd.lng[p], p, ctx->d_scratch, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        free_links(ctx, p);
+        set_last_error(std::string("kq_prepare_links: ") + cudaGetErrorString(e));
+        return status_of(e);
+    }
+    ctx->gd.have[p] = true;
+    return KUQCD_SUCCESS;
+}
+
+KQ_API size_t kq_spinor_bytes(const kq_context *ctx, int prec)
+{
+    const int p = prec_from_api(prec);
+    if (!ctx || p < 0) return 0;
+    return spinor_bytes(ctx->g, p);
+}
+
+KQ_API KuQCDStatus kq_spinor_upload(kq_context *ctx, int prec, const void *host, int host_prec, void *d_field,
+                                    void *stream)
+{
+    if (!ctx || !host || !d_field) return KUQCD_ERR_NULL_POINTER;
+    const int p = prec_from_api(prec), rp = prec_from_api(host_prec);
+    if (p < 0 || (rp != P64 && rp != P32)) return KUQCD_ERR_INVALID_PARAM;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = pick_stream(ctx, stream);
+    const size_t rb = (size_t)ctx->g.vh * 6 * (rp == P64 ? 8 : 4);
+    void *stage = nullptr;
+    cudaError_t e = cudaMallocAsync(&stage, rb, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(stage, host, rb, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = spinor_from_record(ctx->g, stage, rp, d_field, p, s);
+    if (stage) cudaFreeAsync(stage, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) set_last_error(std::string("kq_spinor_upload: ") + cudaGetErrorString(e));
+    return status_of(e);
+}
+
+KQ_API KuQCDStatus kq_spinor_download(kq_context *ctx, int prec, const void *d_field, void *host, int host_prec,
+                                      void *stream)
+{
+    if (!ctx || !host || !d_field) return KUQCD_ERR_NULL_POINTER;
+    const int p = prec_from_api(prec), rp = prec_from_api(host_prec);
+    if (p < 0 || (rp != P64 && rp != P32)) return KUQCD_ERR_INVALID_PARAM;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = pick_stream(ctx, stream);
+    const size_t rb = (size_t)ctx->g.vh * 6 * (rp == P64 ? 8 : 4);
+    void *stage = nullptr;
+    cudaError_t e = cudaMallocAsync(&stage, rb, s);
+    if (e == cudaSuccess) e = spinor_to_record(ctx->g, d_field, p, stage, rp, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, stage, rb, cudaMemcpyDeviceToHost, s);
+    if (stage) cudaFreeAsync(stage, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) set_last_error(std::string("kq_spinor_download: ") + cudaGetErrorString(e));
+    return status_of(e);
+}
+
+KQ_API KuQCDStatus kq_spinor_convert(kq_context *ctx, const void *d_src, int src_prec, void *d_dst, int dst_prec,
+                                     void *stream)
+{
+    if (!ctx || !d_src || !d_dst) return KUQCD_ERR_NULL_POINTER;
+    const int a = prec_from_api(src_prec), b = prec_from_api(dst_prec);
+    if (a < 0 || b < 0) return KUQCD_ERR_INVALID_PARAM;
+    cudaSetDevice(ctx->device);
+    return status_of(spinor_convert(ctx->g, d_src, a, d_dst, b, pick_stream(ctx, stream)));
+}
+
+KQ_API KuQCDStatus kq_dslash(kq_context *ctx, int prec, const void *d_src, void *d_dst, int dst_parity, void *stream)
+{
+    if (!ctx || !d_src || !d_dst) return KUQCD_ERR_NULL_POINTER;
+    const int p = prec_from_api(prec);
+    if (p < 0 || (dst_parity != 0 && dst_parity != 1)) return KUQCD_ERR_INVALID_PARAM;
+    if (!ctx->gd.have[p]) {
+        KuQCDStatus st = kq_prepare_links(ctx, prec);
+        if (st != KUQCD_SUCCESS) return st;
+    }
+    cudaSetDevice(ctx->device);
+    return status_of(launch_dslash(ctx->g, ctx->gd, p, d_src, d_dst, dst_parity, pick_stream(ctx, stream), 0));
+}
+
+KQ_API KuQCDStatus kq_mdagm(kq_context *ctx, int prec, double sigma, const void *d_src, void *d_dst, void *d_tmp,
+                            int parity, void *stream)
+{
+    if (!ctx || !d_src || !d_dst || !d_tmp) return KUQCD_ERR_NULL_POINTER;
+    const int p = prec_from_api(prec);
+    if (p < 0 || (parity != 0 && parity != 1)) return KUQCD_ERR_INVALID_PARAM;
+    if (!ctx->gd.have[p]) {
+        KuQCDStatus st = kq_prepare_links(ctx, prec);
+        if (st != KUQCD_SUCCESS) return st;
+    }
+    cudaSetDevice(ctx->device);
+    return status_of(launch_mdagm(ctx->g, ctx->gd, p, sigma, d_src, d_tmp, d_dst, parity, pick_stream(ctx, stream)));
+}
+
+KQ_API KuQCDStatus kq_make_links_record(kq_context *ctx, double eps, uint64_t seed, double *d_fat, double *d_long)
+{
+    if (!ctx || !d_fat || !d_long) return KUQCD_ERR_NULL_POINTER;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = make_links_record(ctx->g, eps, seed, d_fat, d_long, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    return status_of(e);
+}
+
+KQ_API KuQCDStatus kq_make_source_record(kq_context *ctx, int parity, uint64_t seed, double *d_b)
+{
+    if (!ctx || !d_b) return KUQCD_ERR_NULL_POINTER;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = make_source_record(ctx->g, parity, seed, d_b, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    return status_of(e);
+}
+
+// ------------------------------------------------------------------------------------------------ solver
+static void absolute_shifts(const kq_solve_param *p, double *out)
+{
+    for (int k = 0; k < p->num_shift; ++k)
+        out[k] = (p->shift_mode == 0 && k > 0) ? p->shifts[0] + p->shifts[k] : p->shifts[k];
+}
+
+static KuQCDStatus check_solve_param(const kq_context *ctx, const kq_solve_param *p)
+{
+    if (!ctx || !p || !p->shifts) {
+        set_last_error("solve: null pointer");
+        return KUQCD_ERR_NULL_POINTER;
+    }
+    if (p->num_shift <= 0 || p->num_shift > kMaxShift) {
+        set_last_error("solve: num_shift must be in 1..64");
+        return KUQCD_ERR_INVALID_PARAM;
+    }
+    if (p->parity != 0 && p->parity != 1) {
+        set_last_error("solve: parity must be 0 or 1");
+        return KUQCD_ERR_INVALID_PARAM;
+    }
+    if (!ctx->fat_loaded || !ctx->long_loaded) {
+        set_last_error("solve: load the fat and long links first");
+        return KUQCD_ERR_UNEXPECTED_CALL_ORDER;
+    }
+    return KUQCD_SUCCESS;
+}
+
+KQ_API KuQCDStatus kq_true_residuals(kq_context *ctx, int parity, int num_shift, const double *sigma,
+                                     const void *d_b, const void *d_x, double *out)
+{
+    if (!ctx || !sigma || !d_b || !d_x || !out) return KUQCD_ERR_NULL_POINTER;
+    if (num_shift < 1 || num_shift > kMaxShift || (parity != 0 && parity != 1)) return KUQCD_ERR_INVALID_PARAM;
+    if (!ctx->gd.have[P64]) {
+        KuQCDStatus st = kq_prepare_links(ctx, KUQCD_DOUBLE);
+        if (st != KUQCD_SUCCESS) return st;
+    }
+    cudaSetDevice(ctx->device);
+    const size_t vb = spinor_bytes(ctx->g, P64);
+    const int nb = (ctx->g.vh + 255) / 256;
+    Carve c(nullptr);
+    c.take(vb);
+    c.take(vb);
+    c.take(sizeof(double) * 2 * nb);
+    cudaError_t e = ensure_work(ctx, c.off);
+    if (e != cudaSuccess) return status_of(e);
+    Carve w(ctx->work);
+    void *tmp = w.take(vb), *s = w.take(vb);
+    double *partials = static_cast<double *>(w.take(sizeof(double) * 2 * nb));
+    e = true_residuals(ctx->g, ctx->gd, parity, num_shift, sigma, d_b, d_x, vb, tmp, s, partials, out, ctx->stream);
+    return status_of(e);
+}
+
+KQ_API KuQCDStatus kq_solve_multishift_device(kq_context *ctx, const kq_solve_param *p, const void *d_b, void *d_x,
+                                              kq_solve_info *info)
+{
+    KuQCDStatus st = check_solve_param(ctx, p);
+    if (st != KUQCD_SUCCESS) return st;
+    if (!d_b || !d_x) return KUQCD_ERR_NULL_POINTER;
+    cudaSetDevice(ctx->device);
+    double sig[kMaxShift];
+    absolute_shifts(p, sig);
+    kq_solve_info local;
+    if (!info) info = &local;
+    memset(info, 0, sizeof(*info));
+    info->num_shift = p->num_shift;
+
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, ctx->stream);
+    cudaError_t e = cudaSuccess;
+    if (p->solver == KQ_SOLVER_MIXED) {
+        e = mixed_solve(ctx, p, sig, d_b, d_x, info);
+    } else {
+        const int prec = prec_from_api(p->prec);
+        if (prec != P64 && prec != P32) {
+            set_last_error("solve: KQ_SOLVER_CGM runs in DOUBLE or SINGLE");
+            return KUQCD_ERR_INVALID_PARAM;
+        }
+        if (!ctx->gd.have[prec]) {
+            st = kq_prepare_links(ctx, p->prec);
+            if (st != KUQCD_SUCCESS) return st;
+        }
+        const Geom &g = ctx->g;
+        const size_t vb = spinor_bytes(g, prec), vb64 = spinor_bytes(g, P64);
+        const int nb = (g.vh + 255) / 256;
+        const int ns = p->num_shift;
+        auto layout = [&](Carve &c, CgmBuffers &w) {
+            w.vec_bytes = vb;
+            w.r = c.take(vb);
+            w.s = c.take(vb);
+            w.tmp = c.take(vb);
+            w.p = c.take(vb * ns);
+            w.partials = static_cast<double *>(c.take(sizeof(double) * nb));
+            w.state = static_cast<CgmState *>(c.take(sizeof(CgmState)));
+            if (prec != P64) {
+                w.b = c.take(vb);
+                w.x = c.take(vb * ns);
+            } else {
+                w.b = d_b;
+                w.x = d_x;
+            }
+        };
+        CgmBuffers w;
+        Carve probe(nullptr);
+        layout(probe, w);
+        e = ensure_work(ctx, probe.off);
+        if (e != cudaSuccess) return status_of(e);
+        Carve c(ctx->work);
+        layout(c, w);
+        w.poll = ctx->poll;
+        if (prec != P64) e = spinor_convert(g, d_b, P64, const_cast<void *>(w.b), prec, ctx->stream);
+        // reference shift semantics inside the recurrence: shifts[0] absolute, shifts[j] relative
+        double rs[kMaxShift];
+        rs[0] = sig[0];
+        for (int k = 1; k < ns; ++k) rs[k] = sig[k] - sig[0];
+        CgmResult r;
+        if (e == cudaSuccess) e = cgm_solve(g, ctx->gd, prec, w, p->parity, ns, rs, p->tol, p->max_iter, 8, &r, ctx->stream);
+        if (e == cudaSuccess && prec != P64)
+            for (int k = 0; k < ns && e == cudaSuccess; ++k)
+                e = spinor_convert(g, static_cast<char *>(w.x) + k * vb, prec, static_cast<char *>(d_x) + k * vb64,
+                                   P64, ctx->stream);
+        if (e == cudaSuccess) {
+            info->iter = r.iter;
+            info->status = r.status ? r.status : (r.iter >= p->max_iter ? KQ_STATUS_MAXITER : 0);
+        }
+    }
+    cudaEventRecord(e1, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    info->seconds = ms * 1e-3;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) {
+        if (std::string(last_error()).empty()) set_last_error(cudaGetErrorString(e));
+        return status_of(e);
+    }
+    return info->status == KQ_STATUS_BREAKDOWN ? KUQCD_ERR_UNKNOWN_ERROR : KUQCD_SUCCESS;
+}
+
+KQ_API KuQCDStatus kq_solve_multishift(kq_context *ctx, const kq_solve_param *p, const void *host_b,
+                                       void *const *host_x, kq_solve_info *info)
+{
+    KuQCDStatus st = check_solve_param(ctx, p);
+    if (st != KUQCD_SUCCESS) return st;
+    if (!host_b || !host_x) return KUQCD_ERR_NULL_POINTER;
+    for (int k = 0; k < p->num_shift; ++k)
+        if (!host_x[k]) return KUQCD_ERR_NULL_POINTER;
+    const int hp = prec_from_api(p->host_prec);
+    if (hp != P64 && hp != P32) {
+        set_last_error("solve: host precision must be DOUBLE or SINGLE");
+        return KUQCD_ERR_INVALID_PARAM;
+    }
+    cudaSetDevice(ctx->device);
+    const size_t vb = spinor_bytes(ctx->g, P64);
+    const size_t io = (size_t)vb * (1 + p->num_shift);
+    void *io_buf = nullptr;
+    // the device fields for b and x live outside the solver workspace
+    cudaError_t e = cudaMallocAsync(&io_buf, io, ctx->stream);
+    if (e != cudaSuccess) return status_of(e);
+    void *d_b = io_buf, *d_x = static_cast<char *>(io_buf) + vb;
+    st = kq_spinor_upload(ctx, KUQCD_DOUBLE, host_b, p->host_prec, d_b, nullptr);
+    if (st == KUQCD_SUCCESS) st = kq_solve_multishift_device(ctx, p, d_b, d_x, info);
+    if (st == KUQCD_SUCCESS || st == KUQCD_ERR_UNKNOWN_ERROR)
+        for (int k = 0; k < p->num_shift; ++k) {
+            KuQCDStatus s2 = kq_spinor_download(ctx, KUQCD_DOUBLE, static_cast<char *>(d_x) + k * vb, host_x[k],
+                                                p->host_prec, nullptr);
+            if (s2 != KUQCD_SUCCESS) st = s2;
+        }
+    cudaFreeAsync(io_buf, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    return st;
+}

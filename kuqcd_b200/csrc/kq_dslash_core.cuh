@@ -1,0 +1,168 @@
+// The HISQ even-odd hopping term for one output site, shared by every kernel that applies it.
+//
+//   (D v)(x) = sum_mu [ F_mu(x) v(x+mu) + L_mu(x) v(x+3mu) - F_mu(x-mu)^dag v(x-mu) - L_mu(x-3mu)^dag v(x-3mu) ]
+//
+// with the reference's factors 1/2 and c3 = -1/48 already folded into the device links (dirac_hisq.cpp:464-502,
+// dirac_hisq.cpp:40).  Output sites have parity p; neighbours are read from the parity-(1-p) field at their
+// checkerboard index, with periodic wrap in every direction (Position::Normalize, space_time.cpp:187-197); the
+// backward links live at the neighbour site on the other parity (dirac_hisq.cpp:492,499).
+#pragma once
+#include "kq_internal.h"
+#include "kq_prec.cuh"
+
+namespace kq {
+
+// Periodic coordinate for hops of at most 3 (any extent >= 1, so nt = 1 wraps onto itself as in the reference).
+__device__ __forceinline__ int wrap3(int v, int n)
+{
+    if (n > 3) return v < 0 ? v + n : (v >= n ? v - n : v);
+    v %= n;
+    return v < 0 ? v + n : v;
+}
+
+template <typename T>
+__device__ __forceinline__ void mv_add(const T u[18], const T v[6], T acc[6])
+{
+    // acc += U v, U row-major
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        T re = acc[2 * r], im = acc[2 * r + 1];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const T ur = u[2 * (c + 3 * r)], ui = u[2 * (c + 3 * r) + 1];
+            re += ur * v[2 * c] - ui * v[2 * c + 1];
+            im += ur * v[2 * c + 1] + ui * v[2 * c];
+        }
+        acc[2 * r] = re;
+        acc[2 * r + 1] = im;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void mdv_sub(const T u[18], const T v[6], T acc[6])
+{
+    // acc -= U^dag v : (U^dag v)_r = sum_c conj(U_cr) v_c
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        T re = acc[2 * r], im = acc[2 * r + 1];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const T ur = u[2 * (r + 3 * c)], ui = u[2 * (r + 3 * c) + 1];
+            re -= ur * v[2 * c] + ui * v[2 * c + 1];
+            im -= ur * v[2 * c + 1] - ui * v[2 * c];
+        }
+        acc[2 * r] = re;
+        acc[2 * r + 1] = im;
+    }
+}
+
+// Checkerboard coordinates of output site i on parity p.
+struct SiteCoord {
+    int x, y, z, t, xcb;
+};
+
+__device__ __forceinline__ SiteCoord site_coord(const Geom &g, int i, int p)
+{
+    SiteCoord c;
+    int r = i / g.hx;
+    c.xcb = i - r * g.hx;
+    const int r2 = r / g.n[1];
+    c.y = r - r2 * g.n[1];
+    c.t = r2 / g.n[2];
+    c.z = r2 - c.t * g.n[2];
+    c.x = 2 * c.xcb + ((c.y + c.z + c.t + p) & 1);
+    return c;
+}
+
+// Neighbour checkerboard index for a hop of `hop` in direction dir.
+__device__ __forceinline__ int nbr_index(const Geom &g, const SiteCoord &c, int i, int dir, int hop)
+{
+    switch (dir) {
+        case 0: return i - c.xcb + (wrap3(c.x + hop, g.n[0]) >> 1);
+        case 1: return i + (wrap3(c.y + hop, g.n[1]) - c.y) * g.sy;
+        case 2: return i + (wrap3(c.z + hop, g.n[2]) - c.z) * g.sz;
+        default: return i + (wrap3(c.t + hop, g.n[3]) - c.t) * g.st;
+    }
+}
+
+// acc = (D src)(i) for output parity p.  src is the parity-(1-p) field.
+template <int P>
+__device__ __forceinline__ void dslash_site(const Geom &g, int pv, const LinkSet &fat, const LinkSet &lng,
+                                            const void *src, int p, int i, typename Acc<P>::T acc[6])
+{
+    using T = typename Acc<P>::T;
+    const SiteCoord c = site_coord(g, i, p);
+    // select parity planes without indexing the parameter arrays dynamically (keeps them out of local memory)
+    const void *fat_p = p ? fat.par[1] : fat.par[0], *fat_q = p ? fat.par[0] : fat.par[1];
+    const void *lng_p = p ? lng.par[1] : lng.par[0], *lng_q = p ? lng.par[0] : lng.par[1];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) acc[k] = T(0);
+#pragma unroll
+    for (int dir = 0; dir < 4; ++dir) {
+        const int nf1 = nbr_index(g, c, i, dir, 1);
+        const int nf3 = nbr_index(g, c, i, dir, 3);
+        const int nb1 = nbr_index(g, c, i, dir, -1);
+        const int nb3 = nbr_index(g, c, i, dir, -3);
+        T u[18], v[6];
+        ld_link<P>(fat_p, pv, dir, i, fat.scale, u);
+        ld_spinor<P>(src, pv, nf1, v);
+        mv_add(u, v, acc);
+        ld_link<P>(lng_p, pv, dir, i, lng.scale, u);
+        ld_spinor<P>(src, pv, nf3, v);
+        mv_add(u, v, acc);
+        ld_link<P>(fat_q, pv, dir, nb1, fat.scale, u);
+        ld_spinor<P>(src, pv, nb1, v);
+        mdv_sub(u, v, acc);
+        ld_link<P>(lng_q, pv, dir, nb3, lng.scale, u);
+        ld_spinor<P>(src, pv, nb3, v);
+        mdv_sub(u, v, acc);
+    }
+}
+
+// ------------------------------------------------------------------------------------------------ reductions
+// Deterministic block sum of a double (fixed shuffle tree, then warp 0 over the per-warp sums).
+__device__ __forceinline__ double block_sum(double v, double *smem32)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) smem32[w] = v;
+    __syncthreads();
+    const int nw = (blockDim.x + 31) >> 5;
+    v = (threadIdx.x < nw) ? smem32[threadIdx.x] : 0.0;
+    if (w == 0) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    return v;  // valid in thread 0
+}
+
+// Publish this block's partial sum; returns true in exactly one thread of the last block to arrive, after which
+// *total holds the fixed-order sum of all partials.  Every block calls this unconditionally.
+__device__ __forceinline__ bool grid_sum_last(double v, double *partials, unsigned *ticket, double *smem32,
+                                              double *total)
+{
+    __shared__ bool am_last;
+    v = block_sum(v, smem32);
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = v;
+        __threadfence();
+        const unsigned t = atomicAdd(ticket, 1u);
+        am_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!am_last) return false;
+    __threadfence();
+    double s = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) s += *((volatile double *)partials + b);
+    s = block_sum(s, smem32);
+    if (threadIdx.x == 0) {
+        *total = s;
+        *ticket = 0u;
+        return true;
+    }
+    return false;
+}
+
+}  // namespace kq

@@ -1,0 +1,265 @@
+"""ctypes bindings of libkuqcd_b200.so (declarations in include/kuqcd_b200.h and include/kuqcd.h).
+
+Host-side mirror of the reference API (kuqcd.h:29-34, kuqcd_enum.h:15-121): same enum values, same parameter
+structs, same status codes and call order.  Arrays are numpy arrays in the reference's NORMAL_ORDER host layouts
+(kuqcd.cpp:103-169).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+# ---------------------------------------------------------------- enums (kuqcd_enum.h:15-98 of the reference)
+KUQCD_SUCCESS = 0
+KUQCD_ERR_INVALID_PARAM = -1
+KUQCD_ERR_UNSUPPORTED = -2
+KUQCD_ERR_NULL_POINTER = -3
+KUQCD_ERR_NO_MEMORY = -4
+KUQCD_ERR_UNKNOWN_TYPE = -5
+KUQCD_ERR_UNEXPECTED_CALL_ORDER = -6
+KUQCD_ERR_NO_RESOURCE = -7
+KUQCD_ERR_UNKNOWN_ERROR = -8
+KUQCD_EVEN, KUQCD_ODD, KUQCD_ALL = 0, 1, 2
+KUQCD_HALF, KUQCD_SINGLE, KUQCD_DOUBLE = 2, 4, 8
+KUQCD_XYZT_ORDER, KUQCD_TZYX_ORDER = 0, 1
+KUQCD_NORMAL_ORDER, KUQCD_BATCH_ORDER = 0, 1
+KUQCD_EVEN_EVEN, KUQCD_ODD_ODD = 0, 1
+KUQCD_WILSON_LINK, KUQCD_FAT_LINK, KUQCD_LONG_LINK = 0, 1, 2
+KUQCD_GAUGE_RECON_NO, KUQCD_GAUGE_RECON_U14, KUQCD_GAUGE_RECON_12, KUQCD_GAUGE_RECON_8 = 18, 14, 12, 8
+KUQCD_WILSON_DIRAC, KUQCD_WILSONPC_DIRAC, KUQCD_HISQ_DIRAC, KUQCD_HISQPC_DIRAC = 0, 1, 2, 3
+KUQCD_CG, KUQCD_CGM = 0, 1
+KQ_SOLVER_CGM, KQ_SOLVER_MIXED = 0, 1
+
+
+class KuQCDGaugeParam(C.Structure):
+    _fields_ = [("lat", C.c_uint * 4), ("halo_depth", C.c_int), ("od", C.c_int), ("site_subset", C.c_int),
+                ("gauge_order", C.c_int), ("prec", C.c_int), ("link_type", C.c_int), ("recon", C.c_int)]
+
+
+class KuQCDInvertParam(C.Structure):
+    _fields_ = [("dslash_type", C.c_int), ("inverter_type", C.c_int), ("matpc_type", C.c_int), ("prec", C.c_int),
+                ("num_shift", C.c_int), ("max_iter", C.c_int), ("iter", C.c_int), ("tol", C.c_double),
+                ("shifts", C.POINTER(C.c_double))]
+
+
+class SolveParam(C.Structure):
+    _fields_ = [("parity", C.c_int), ("num_shift", C.c_int), ("shifts", C.POINTER(C.c_double)),
+                ("shift_mode", C.c_int), ("solver", C.c_int), ("prec", C.c_int), ("host_prec", C.c_int),
+                ("max_iter", C.c_int), ("tol", C.c_double), ("rel_residual", C.c_double)]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("iter", C.c_int), ("iter_refine", C.c_int), ("status", C.c_int), ("num_shift", C.c_int),
+                ("true_residual", C.c_double * 64), ("seconds", C.c_double)]
+
+
+# every symbol include/*.h declares for the C ABI (checked by the CPU test suite)
+EXPORTED_SYMBOLS = [
+    "kq_kuqcd_init", "kq_kuqcd_load_gaugefield", "kq_kuqcd_solve_multishift", "kq_kuqcd_gauge_free",
+    "kq_kuqcd_end", "kq_context_create", "kq_context_destroy", "kq_load_links", "kq_prepare_links",
+    "kq_spinor_bytes", "kq_spinor_upload", "kq_spinor_download", "kq_spinor_convert", "kq_dslash", "kq_mdagm",
+    "kq_solve_multishift", "kq_solve_multishift_device", "kq_true_residuals", "kq_make_links_record",
+    "kq_make_source_record", "kq_last_error",
+]
+
+_PKG = Path(__file__).resolve().parent
+lib_path = Path(os.environ.get("KUQCD_B200_LIB", _PKG / "libkuqcd_b200.so"))
+_lib = None
+
+
+class KuQCDError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        msg = library().kq_last_error().decode(errors="replace")
+        super().__init__(f"{where} failed with status {status}: {msg}")
+        self.status = status
+
+
+def library() -> C.CDLL:
+    """Load libkuqcd_b200.so (raises if it has not been built: there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not lib_path.exists():
+        raise RuntimeError(f"{lib_path} is missing: build it with `python -m kuqcd_b200.build`")
+    L = C.CDLL(str(lib_path))
+    vp, i, u, d, sz = C.c_void_p, C.c_int, C.c_uint, C.c_double, C.c_size_t
+    sig = {
+        "kq_kuqcd_init": (i, []),
+        "kq_kuqcd_load_gaugefield": (i, [vp, C.POINTER(KuQCDGaugeParam)]),
+        "kq_kuqcd_solve_multishift": (i, [C.POINTER(vp), vp, C.POINTER(KuQCDInvertParam)]),
+        "kq_kuqcd_gauge_free": (None, []),
+        "kq_kuqcd_end": (None, []),
+        "kq_context_create": (i, [C.POINTER(u), i, C.POINTER(vp)]),
+        "kq_context_destroy": (None, [vp]),
+        "kq_load_links": (i, [vp, i, vp, i]),
+        "kq_prepare_links": (i, [vp, i]),
+        "kq_spinor_bytes": (sz, [vp, i]),
+        "kq_spinor_upload": (i, [vp, i, vp, i, vp, vp]),
+        "kq_spinor_download": (i, [vp, i, vp, vp, i, vp]),
+        "kq_spinor_convert": (i, [vp, vp, i, vp, i, vp]),
+        "kq_dslash": (i, [vp, i, vp, vp, i, vp]),
+        "kq_mdagm": (i, [vp, i, d, vp, vp, vp, i, vp]),
+        "kq_solve_multishift": (i, [vp, C.POINTER(SolveParam), vp, C.POINTER(vp), C.POINTER(SolveInfo)]),
+        "kq_solve_multishift_device": (i, [vp, C.POINTER(SolveParam), vp, vp, C.POINTER(SolveInfo)]),
+        "kq_true_residuals": (i, [vp, i, i, C.POINTER(d), vp, vp, C.POINTER(d)]),
+        "kq_make_links_record": (i, [vp, d, C.c_uint64, vp, vp]),
+        "kq_make_source_record": (i, [vp, i, C.c_uint64, vp]),
+        "kq_last_error": (C.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _ptr(a) -> C.c_void_p:
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return C.c_void_p(a)
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _np_prec(a: np.ndarray) -> int:
+    if a.dtype == np.float64:
+        return KUQCD_DOUBLE
+    if a.dtype == np.float32:
+        return KUQCD_SINGLE
+    raise TypeError(f"host records are float64 or float32, not {a.dtype}")
+
+
+# ---------------------------------------------------------------- reference-facing calls (kuqcd.h:29-34)
+def kuqcd_init() -> int:
+    return library().kq_kuqcd_init()
+
+
+def kuqcd_load_gaugefield(h_gauge, param: KuQCDGaugeParam) -> int:
+    return library().kq_kuqcd_load_gaugefield(_ptr(h_gauge), C.byref(param) if param is not None else None)
+
+
+def kuqcd_solve_multishift(hp_x, hp_b, param: KuQCDInvertParam) -> int:
+    xs = None
+    if hp_x is not None:
+        xs = (C.c_void_p * len(hp_x))(*[_ptr(x).value if x is not None else None for x in hp_x])
+    return library().kq_kuqcd_solve_multishift(xs, _ptr(hp_b), C.byref(param) if param is not None else None)
+
+
+def kuqcd_gauge_free() -> None:
+    library().kq_kuqcd_gauge_free()
+
+
+def kuqcd_end() -> None:
+    library().kq_kuqcd_end()
+
+
+# ---------------------------------------------------------------- device-level API
+class Context:
+    """One lattice on one GPU (kq_context): device links, stream, solver workspace."""
+
+    def __init__(self, lat, device: int = 0):
+        self.lat = tuple(int(v) for v in lat)
+        self.V = int(np.prod(self.lat))
+        self.Vh = self.V // 2
+        L = library()
+        h = C.c_void_p()
+        st = L.kq_context_create((C.c_uint * 4)(*self.lat), device, C.byref(h))
+        if st != 0:
+            raise KuQCDError(st, "kq_context_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library().kq_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, st, where):
+        if st != 0:
+            raise KuQCDError(st, where)
+
+    def load_links(self, link_type: int, host: np.ndarray):
+        host = np.ascontiguousarray(host)
+        assert host.size == self.V * 72, "gauge record has V*4*18 reals"
+        self._chk(library().kq_load_links(self._h, link_type, _ptr(host), _np_prec(host)), "kq_load_links")
+
+    def prepare(self, prec: int):
+        self._chk(library().kq_prepare_links(self._h, prec), "kq_prepare_links")
+
+    def spinor_bytes(self, prec: int) -> int:
+        return int(library().kq_spinor_bytes(self._h, prec))
+
+    def upload(self, prec: int, host: np.ndarray, dev, stream=None):
+        host = np.ascontiguousarray(host)
+        self._chk(library().kq_spinor_upload(self._h, prec, _ptr(host), _np_prec(host), _ptr(dev), stream),
+                  "kq_spinor_upload")
+
+    def download(self, prec: int, dev, host_dtype=np.float64, stream=None) -> np.ndarray:
+        out = np.empty(self.Vh * 6, dtype=host_dtype)
+        self._chk(library().kq_spinor_download(self._h, prec, _ptr(dev), _ptr(out), _np_prec(out), stream),
+                  "kq_spinor_download")
+        return out
+
+    def convert(self, src, src_prec: int, dst, dst_prec: int, stream=None):
+        self._chk(library().kq_spinor_convert(self._h, _ptr(src), src_prec, _ptr(dst), dst_prec, stream),
+                  "kq_spinor_convert")
+
+    def dslash(self, prec: int, src, dst, dst_parity: int, stream=None):
+        self._chk(library().kq_dslash(self._h, prec, _ptr(src), _ptr(dst), dst_parity, stream), "kq_dslash")
+
+    def mdagm(self, prec: int, sigma: float, src, dst, tmp, parity: int, stream=None):
+        self._chk(library().kq_mdagm(self._h, prec, sigma, _ptr(src), _ptr(dst), _ptr(tmp), parity, stream),
+                  "kq_mdagm")
+
+    @staticmethod
+    def _param(shifts, parity, solver, prec, host_prec, max_iter, tol, rel_residual, shift_mode):
+        sh = (C.c_double * len(shifts))(*[float(s) for s in shifts])
+        p = SolveParam(parity=parity, num_shift=len(shifts), shifts=C.cast(sh, C.POINTER(C.c_double)),
+                       shift_mode=shift_mode, solver=solver, prec=prec, host_prec=host_prec, max_iter=max_iter,
+                       tol=tol, rel_residual=rel_residual)
+        return p, sh
+
+    def solve(self, b: np.ndarray, shifts, parity=0, solver=KQ_SOLVER_CGM, prec=KUQCD_DOUBLE, max_iter=10000,
+              tol=0.0, rel_residual=1e-10, shift_mode=1):
+        """Host b -> list of host x (dtype of b).  shift_mode 1: absolute shifts, 0: reference semantics."""
+        b = np.ascontiguousarray(b)
+        xs = [np.zeros_like(b) for _ in shifts]
+        p, keep = self._param(shifts, parity, solver, prec, _np_prec(b), max_iter, tol, rel_residual, shift_mode)
+        info = SolveInfo()
+        xp = (C.c_void_p * len(xs))(*[x.ctypes.data for x in xs])
+        st = library().kq_solve_multishift(self._h, C.byref(p), _ptr(b), xp, C.byref(info))
+        self._chk(st, "kq_solve_multishift")
+        return xs, info
+
+    def solve_device(self, d_b, d_x, shifts, parity=0, solver=KQ_SOLVER_CGM, prec=KUQCD_DOUBLE, max_iter=10000,
+                     tol=0.0, rel_residual=1e-10, shift_mode=1):
+        p, keep = self._param(shifts, parity, solver, prec, KUQCD_DOUBLE, max_iter, tol, rel_residual, shift_mode)
+        info = SolveInfo()
+        self._chk(library().kq_solve_multishift_device(self._h, C.byref(p), _ptr(d_b), _ptr(d_x), C.byref(info)),
+                  "kq_solve_multishift_device")
+        return info
+
+    def true_residuals(self, parity, sigmas, d_b, d_x):
+        sg = (C.c_double * len(sigmas))(*[float(s) for s in sigmas])
+        out = (C.c_double * len(sigmas))()
+        self._chk(library().kq_true_residuals(self._h, parity, len(sigmas), sg, _ptr(d_b), _ptr(d_x), out),
+                  "kq_true_residuals")
+        return list(out)
+
+    def make_links(self, eps: float, seed: int, d_fat, d_long):
+        self._chk(library().kq_make_links_record(self._h, eps, seed, _ptr(d_fat), _ptr(d_long)),
+                  "kq_make_links_record")
+
+    def make_source(self, parity: int, seed: int, d_b):
+        self._chk(library().kq_make_source_record(self._h, parity, seed, _ptr(d_b)), "kq_make_source_record")
