@@ -99,6 +99,8 @@ typedef struct {
     int num_shift;
     double true_residual[64]; /* |b - (sigma_k - DD) x_k| / |b| in FP64, when computed */
     double seconds;           /* device time of the solve */
+    long long kernel_launches;/* kernels the solve enqueued (graph nodes included) */
+    double sloppy_residual;   /* KQ_SOLVER_MIXED: largest true relative residual after the sloppy multishift */
 } kq_solve_info;
 
 /* Host b (num Vh*6 values of host_prec) -> host x[k].  Copies in, solves on the device, copies out. */

@@ -8,6 +8,7 @@
 #include <string>
 #include <vector>
 
+#include "kq_context.h"
 #include "kq_internal.h"
 #include "kq_prec.cuh"
 #include "kq_solver.h"
@@ -31,36 +32,7 @@ cudaError_t true_residuals(const Geom &g, const GaugeDev &gd, int parity, int ns
 using namespace kq;
 
 // ------------------------------------------------------------------------------------------------ context
-struct kq_context {
-    int device = 0;
-    unsigned lat[4] = {0, 0, 0, 0};
-    Geom g{};
-    cudaStream_t stream = nullptr;
-    GaugeDev gd;
-    int master = -1;  // precision of the loaded links (P64 or P32)
-    bool fat_loaded = false, long_loaded = false;
-    unsigned *d_scratch = nullptr;
-    // solver workspace (grown on demand)
-    void *work = nullptr;
-    size_t work_bytes = 0;
-    CgmPoll *poll = nullptr;  // pinned
-};
-
 namespace kq {
-
-// Workspace carving helper: 256-byte aligned bump allocator over ctx->work.
-struct Carve {
-    char *base;
-    size_t off = 0;
-    explicit Carve(void *b) : base(static_cast<char *>(b)) {}
-    void *take(size_t n)
-    {
-        off = (off + 255) & ~size_t(255);
-        void *p = base ? base + off : nullptr;
-        off += n;
-        return p;
-    }
-};
 
 cudaError_t ensure_work(::kq_context *ctx, size_t bytes)
 {
@@ -466,13 +438,14 @@ KQ_API KuQCDStatus kq_solve_multishift_device(kq_context *ctx, const kq_solve_pa
         rs[0] = sig[0];
         for (int k = 1; k < ns; ++k) rs[k] = sig[k] - sig[0];
         CgmResult r;
-        if (e == cudaSuccess) e = cgm_solve(g, ctx->gd, prec, w, p->parity, ns, rs, p->tol, p->max_iter, 8, &r, ctx->stream);
+        if (e == cudaSuccess) e = cgm_solve(g, ctx->gd, prec, prec, w, p->parity, ns, rs, p->tol, p->max_iter, 8, &r, ctx->stream);
         if (e == cudaSuccess && prec != P64)
             for (int k = 0; k < ns && e == cudaSuccess; ++k)
                 e = spinor_convert(g, static_cast<char *>(w.x) + k * vb, prec, static_cast<char *>(d_x) + k * vb64,
                                    P64, ctx->stream);
         if (e == cudaSuccess) {
             info->iter = r.iter;
+            info->kernel_launches = r.launches + (prec != P64 ? 1 + ns : 0);
             info->status = r.status ? r.status : (r.iter >= p->max_iter ? KQ_STATUS_MAXITER : 0);
         }
     }

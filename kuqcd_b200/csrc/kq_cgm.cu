@@ -20,7 +20,7 @@
 
 namespace kq {
 
-cudaError_t launch_dslash_gated(const Geom &g, const GaugeDev &gd, int prec, const void *src, void *dst,
+cudaError_t launch_dslash_gated(const Geom &g, const GaugeDev &gd, int lp, int sp, const void *src, void *dst,
                                 int dst_parity, const int *gate, cudaStream_t s);
 
 // ------------------------------------------------------------------------------------------------ scalar steps
@@ -108,8 +108,8 @@ __global__ void __launch_bounds__(256) cgm_init_kernel(int vh, int pv, const voi
     }
 }
 
-// s = shifts[0] * p0 - D tmp ; pAp = Re<p0, s>
-template <int P>
+// s = shifts[0] * p0 - D tmp ; pAp = Re<p0, s>   (links LP, vectors P)
+template <int LP, int P>
 __global__ void __launch_bounds__(256) cgm_dslash2_kernel(Geom g, int pv, LinkSet fat, LinkSet lng,
                                                           const void *__restrict__ tmp, const void *__restrict__ p0,
                                                           void *__restrict__ s, int p, CgmState *st, double *partials)
@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(256) cgm_dslash2_kernel(Geom g, int pv, LinkSe
     double dot = 0.0;
     if (i < g.vh) {
         T acc[6], pv6[6];
-        dslash_site<P>(g, pv, fat, lng, tmp, p, i, acc);
+        dslash_site2<LP, P>(g, pv, fat, lng, tmp, p, i, acc);
         ld_spinor<P>(p0, pv, i, pv6);
         const T sig = (T)st->shift[0];
 #pragma unroll
@@ -206,22 +206,27 @@ __global__ void __launch_bounds__(256) cgm_xp_kernel(int vh, int pv, const void 
 }
 
 // ------------------------------------------------------------------------------------------------ driver
-template <int P>
+template <int LP, int P>
 static cudaError_t enqueue_iteration(const Geom &g, const GaugeDev &gd, const CgmBuffers &w, int parity,
                                      CgmState *st, cudaStream_t s)
 {
     const int pv = pad_sites(g.vh);
     const int bs = 256, nb = (g.vh + bs - 1) / bs;
-    KQ_CUDA_TRY(launch_dslash_gated(g, gd, P, w.p, w.tmp, 1 - parity, &st->active, s));
-    cgm_dslash2_kernel<P><<<nb, bs, 0, s>>>(g, pv, gd.fat[P], gd.lng[P], w.tmp, w.p, w.s, parity, st, w.partials);
+    KQ_CUDA_TRY(launch_dslash_gated(g, gd, LP, P, w.p, w.tmp, 1 - parity, &st->active, s));
+    cgm_dslash2_kernel<LP, P><<<nb, bs, 0, s>>>(g, pv, gd.fat[LP], gd.lng[LP], w.tmp, w.p, w.s, parity, st,
+                                                w.partials);
     cgm_r_kernel<P><<<nb, bs, 0, s>>>(g.vh, pv, w.r, w.s, st, w.partials);
     cgm_xp_kernel<P, P><<<nb, bs, 0, s>>>(g.vh, pv, w.r, w.p, w.vec_bytes, w.x, w.vec_bytes, st);
     return cudaGetLastError();
 }
 
-cudaError_t cgm_solve(const Geom &g, const GaugeDev &gd, int prec, const CgmBuffers &w, int parity, int ns,
+cudaError_t cgm_solve(const Geom &g, const GaugeDev &gd, int lp, int prec, const CgmBuffers &w, int parity, int ns,
                       const double *shifts, double tol, int max_iter, int chunk, CgmResult *res, cudaStream_t s)
 {
+    if (!((lp == prec) || (lp == P16 && prec == P32)) || !gd.have[lp]) {
+        set_last_error("cgm: unsupported link/vector precision pair or links not resident");
+        return cudaErrorInvalidValue;
+    }
     if (ns < 1 || ns > kMaxShift) {
         set_last_error("cgm: num_shift out of range (1..64)");
         return cudaErrorInvalidValue;
@@ -255,8 +260,9 @@ cudaError_t cgm_solve(const Geom &g, const GaugeDev &gd, int prec, const CgmBuff
     KQ_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     cudaError_t ce = cudaSuccess;
     for (int c = 0; c < chunk && ce == cudaSuccess; ++c)
-        ce = prec == P64 ? enqueue_iteration<0>(g, gd, w, parity, w.state, cs)
-                         : enqueue_iteration<1>(g, gd, w, parity, w.state, cs);
+        ce = prec == P64  ? enqueue_iteration<0, 0>(g, gd, w, parity, w.state, cs)
+             : lp == P32 ? enqueue_iteration<1, 1>(g, gd, w, parity, w.state, cs)
+                         : enqueue_iteration<2, 1>(g, gd, w, parity, w.state, cs);
     cudaError_t ee = cudaStreamEndCapture(cs, &graph);
     if (ce != cudaSuccess || ee != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
@@ -285,6 +291,7 @@ cudaError_t cgm_solve(const Geom &g, const GaugeDev &gd, int prec, const CgmBuff
     KQ_CUDA_TRY(err);
     KQ_CUDA_TRY(cudaMemcpyAsync(&h, w.state, sizeof(CgmState), cudaMemcpyDeviceToHost, s));
     KQ_CUDA_TRY(cudaStreamSynchronize(s));
+    res->launches = 1 + 4LL * launched;
     res->iter = h.iter;
     res->status = h.status;
     res->rnorm2 = h.rNorm2;

@@ -1,0 +1,40 @@
+// The kq_context object behind the C ABI handle, and the workspace helpers the solvers share.
+#pragma once
+#include "kq_internal.h"
+#include "kq_solver.h"
+
+struct kq_context {
+    int device = 0;
+    unsigned lat[4] = {0, 0, 0, 0};
+    kq::Geom g{};
+    cudaStream_t stream = nullptr;
+    kq::GaugeDev gd;
+    int master = -1;  // precision of the loaded links (P64 or P32)
+    bool fat_loaded = false, long_loaded = false;
+    unsigned *d_scratch = nullptr;
+    // solver workspace (grown on demand, never shrunk)
+    void *work = nullptr;
+    size_t work_bytes = 0;
+    kq::CgmPoll *poll = nullptr;  // pinned host page for state polling
+};
+
+namespace kq {
+
+// 256-byte aligned bump allocator over a workspace; with a null base it only measures.
+struct Carve {
+    char *base;
+    size_t off = 0;
+    explicit Carve(void *b) : base(static_cast<char *>(b)) {}
+    void *take(size_t n)
+    {
+        off = (off + 255) & ~size_t(255);
+        void *p = base ? base + off : nullptr;
+        off += n;
+        return p;
+    }
+};
+
+cudaError_t ensure_work(::kq_context *ctx, size_t bytes);
+KuQCDStatus status_of(cudaError_t e);
+
+}  // namespace kq

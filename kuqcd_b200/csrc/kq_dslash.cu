@@ -1,89 +1,95 @@
 // Stand-alone HISQ even-odd dslash kernels: dst = D src, and s = sigma*p - D src (the second half of
 // sigma - D_pq D_qp, MdaggM + Axmy of inverter_cgm.cpp:45-46).  One thread per output site; links are
-// streamed from HBM once, neighbour spinors come through L1/L2.
+// streamed from HBM once, neighbour spinors come through L1/L2.  Link and spinor precisions are independent
+// template parameters (FP64/FP64, FP32/FP32, HALF/HALF, HALF links with FP32 spinors).
 #include "kq_dslash_core.cuh"
 
 namespace kq {
 
-template <int P>
+template <int LP, int SP>
 __global__ void __launch_bounds__(256) dslash_kernel(Geom g, int pv, LinkSet fat, LinkSet lng, const void *__restrict__ src,
                                                      void *__restrict__ dst, int p, const int *__restrict__ gate)
 {
     if (gate && *gate == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.vh) return;
-    typename Acc<P>::T acc[6];
-    dslash_site<P>(g, pv, fat, lng, src, p, i, acc);
-    st_spinor<P>(dst, pv, i, acc);
+    typename Acc2<LP, SP>::T acc[6];
+    dslash_site2<LP, SP>(g, pv, fat, lng, src, p, i, acc);
+    st_spinor<SP>(dst, pv, i, acc);
 }
 
 // s = sigma * pvec - D src   (pvec, s on parity p)
-template <int P>
+template <int LP, int SP>
 __global__ void __launch_bounds__(256) dslash_xmy_kernel(Geom g, int pv, LinkSet fat, LinkSet lng,
                                                          const void *__restrict__ src, const void *__restrict__ pvec,
                                                          void *__restrict__ s, int p, double sigma)
 {
-    using T = typename Acc<P>::T;
+    using T = typename Acc2<LP, SP>::T;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.vh) return;
     T acc[6], pv6[6];
-    dslash_site<P>(g, pv, fat, lng, src, p, i, acc);
-    ld_spinor<P>(pvec, pv, i, pv6);
+    dslash_site2<LP, SP>(g, pv, fat, lng, src, p, i, acc);
+    ld_spinor<SP>(pvec, pv, i, pv6);
 #pragma unroll
     for (int k = 0; k < 6; ++k) acc[k] = (T)sigma * pv6[k] - acc[k];
-    st_spinor<P>(s, pv, i, acc);
+    st_spinor<SP>(s, pv, i, acc);
 }
 
-cudaError_t launch_dslash(const Geom &g, const GaugeDev &gd, int prec, const void *src, void *dst, int dst_parity,
-                          cudaStream_t s, int block)
+static bool pair_ok(int lp, int sp)
 {
-    if (!gd.have[prec]) {
-        set_last_error("dslash: links not resident in the requested precision");
+    return (lp == sp) || (lp == P16 && sp == P32);
+}
+
+#define KQ_DISPATCH_PAIR(LPv, SPv, CALL)                                   \
+    if (LPv == P64 && SPv == P64) { constexpr int LP = 0, SP = 0; CALL; } \
+    else if (LPv == P32 && SPv == P32) { constexpr int LP = 1, SP = 1; CALL; } \
+    else if (LPv == P16 && SPv == P16) { constexpr int LP = 2, SP = 2; CALL; } \
+    else { constexpr int LP = 2, SP = 1; CALL; }
+
+cudaError_t launch_dslash2(const Geom &g, const GaugeDev &gd, int lp, int sp, const void *src, void *dst,
+                           int dst_parity, const int *gate, cudaStream_t s, int block)
+{
+    if (!gd.have[lp] || !pair_ok(lp, sp)) {
+        set_last_error("dslash: links not resident in the requested precision, or unsupported precision pair");
         return cudaErrorInvalidValue;
     }
     const int bs = block > 0 ? block : 256;
     const int nb = (g.vh + bs - 1) / bs;
     const int pv = pad_sites(g.vh);
-    switch (prec) {
-        case P64: dslash_kernel<0><<<nb, bs, 0, s>>>(g, pv, gd.fat[0], gd.lng[0], src, dst, dst_parity, nullptr); break;
-        case P32: dslash_kernel<1><<<nb, bs, 0, s>>>(g, pv, gd.fat[1], gd.lng[1], src, dst, dst_parity, nullptr); break;
-        default: dslash_kernel<2><<<nb, bs, 0, s>>>(g, pv, gd.fat[2], gd.lng[2], src, dst, dst_parity, nullptr); break;
-    }
+    KQ_DISPATCH_PAIR(lp, sp, (dslash_kernel<LP, SP><<<nb, bs, 0, s>>>(g, pv, gd.fat[lp], gd.lng[lp], src, dst,
+                                                                       dst_parity, gate)));
     return cudaGetLastError();
 }
 
-cudaError_t launch_dslash_gated(const Geom &g, const GaugeDev &gd, int prec, const void *src, void *dst,
+cudaError_t launch_dslash(const Geom &g, const GaugeDev &gd, int prec, const void *src, void *dst, int dst_parity,
+                          cudaStream_t s, int block)
+{
+    return launch_dslash2(g, gd, prec, prec, src, dst, dst_parity, nullptr, s, block);
+}
+
+cudaError_t launch_dslash_gated(const Geom &g, const GaugeDev &gd, int lp, int sp, const void *src, void *dst,
                                 int dst_parity, const int *gate, cudaStream_t s)
 {
+    return launch_dslash2(g, gd, lp, sp, src, dst, dst_parity, gate, s, 0);
+}
+
+cudaError_t launch_mdagm2(const Geom &g, const GaugeDev &gd, int lp, int sp, double sigma, const void *src,
+                          void *tmp, void *dst, int parity, cudaStream_t s)
+{
+    cudaError_t e = launch_dslash2(g, gd, lp, sp, src, tmp, 1 - parity, nullptr, s, 0);
+    if (e != cudaSuccess) return e;
     const int bs = 256;
     const int nb = (g.vh + bs - 1) / bs;
     const int pv = pad_sites(g.vh);
-    switch (prec) {
-        case P64: dslash_kernel<0><<<nb, bs, 0, s>>>(g, pv, gd.fat[0], gd.lng[0], src, dst, dst_parity, gate); break;
-        case P32: dslash_kernel<1><<<nb, bs, 0, s>>>(g, pv, gd.fat[1], gd.lng[1], src, dst, dst_parity, gate); break;
-        default: dslash_kernel<2><<<nb, bs, 0, s>>>(g, pv, gd.fat[2], gd.lng[2], src, dst, dst_parity, gate); break;
-    }
+    KQ_DISPATCH_PAIR(lp, sp, (dslash_xmy_kernel<LP, SP><<<nb, bs, 0, s>>>(g, pv, gd.fat[lp], gd.lng[lp], tmp, src,
+                                                                           dst, parity, sigma)));
     return cudaGetLastError();
 }
 
 cudaError_t launch_mdagm(const Geom &g, const GaugeDev &gd, int prec, double sigma, const void *src, void *tmp,
                          void *dst, int parity, cudaStream_t s)
 {
-    if (!gd.have[prec]) {
-        set_last_error("mdagm: links not resident in the requested precision");
-        return cudaErrorInvalidValue;
-    }
-    cudaError_t e = launch_dslash(g, gd, prec, src, tmp, 1 - parity, s, 0);
-    if (e != cudaSuccess) return e;
-    const int bs = 256;
-    const int nb = (g.vh + bs - 1) / bs;
-    const int pv = pad_sites(g.vh);
-    switch (prec) {
-        case P64: dslash_xmy_kernel<0><<<nb, bs, 0, s>>>(g, pv, gd.fat[0], gd.lng[0], tmp, src, dst, parity, sigma); break;
-        case P32: dslash_xmy_kernel<1><<<nb, bs, 0, s>>>(g, pv, gd.fat[1], gd.lng[1], tmp, src, dst, parity, sigma); break;
-        default: dslash_xmy_kernel<2><<<nb, bs, 0, s>>>(g, pv, gd.fat[2], gd.lng[2], tmp, src, dst, parity, sigma); break;
-    }
-    return cudaGetLastError();
+    return launch_mdagm2(g, gd, prec, prec, sigma, src, tmp, dst, parity, s);
 }
 
 }  // namespace kq

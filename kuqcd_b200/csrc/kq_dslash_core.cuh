@@ -85,12 +85,18 @@ __device__ __forceinline__ int nbr_index(const Geom &g, const SiteCoord &c, int 
     }
 }
 
-// acc = (D src)(i) for output parity p.  src is the parity-(1-p) field.
-template <int P>
-__device__ __forceinline__ void dslash_site(const Geom &g, int pv, const LinkSet &fat, const LinkSet &lng,
-                                            const void *src, int p, int i, typename Acc<P>::T acc[6])
+// Accumulation type of a (link precision, spinor precision) pair: double only when both are FP64.
+template <int LP, int SP> struct Acc2 { using T = float; };
+template <> struct Acc2<0, 0> { using T = double; };
+
+// acc = (D src)(i) for output parity p.  src is the parity-(1-p) field.  Links in precision LP, spinors in SP.
+template <int LP, int SP>
+__device__ __forceinline__ void dslash_site2(const Geom &g, int pv, const LinkSet &fat, const LinkSet &lng,
+                                             const void *src, int p, int i, typename Acc2<LP, SP>::T acc[6])
 {
-    using T = typename Acc<P>::T;
+    using T = typename Acc2<LP, SP>::T;
+    static_assert(sizeof(typename Acc<LP>::T) == sizeof(T) && sizeof(typename Acc<SP>::T) == sizeof(T),
+                  "FP64 links go with FP64 spinors");
     const SiteCoord c = site_coord(g, i, p);
     // select parity planes without indexing the parameter arrays dynamically (keeps them out of local memory)
     const void *fat_p = p ? fat.par[1] : fat.par[0], *fat_q = p ? fat.par[0] : fat.par[1];
@@ -104,18 +110,78 @@ __device__ __forceinline__ void dslash_site(const Geom &g, int pv, const LinkSet
         const int nb1 = nbr_index(g, c, i, dir, -1);
         const int nb3 = nbr_index(g, c, i, dir, -3);
         T u[18], v[6];
-        ld_link<P>(fat_p, pv, dir, i, fat.scale, u);
-        ld_spinor<P>(src, pv, nf1, v);
+        ld_link<LP>(fat_p, pv, dir, i, fat.scale, u);
+        ld_spinor<SP>(src, pv, nf1, v);
         mv_add(u, v, acc);
-        ld_link<P>(lng_p, pv, dir, i, lng.scale, u);
-        ld_spinor<P>(src, pv, nf3, v);
+        ld_link<LP>(lng_p, pv, dir, i, lng.scale, u);
+        ld_spinor<SP>(src, pv, nf3, v);
         mv_add(u, v, acc);
-        ld_link<P>(fat_q, pv, dir, nb1, fat.scale, u);
-        ld_spinor<P>(src, pv, nb1, v);
+        ld_link<LP>(fat_q, pv, dir, nb1, fat.scale, u);
+        ld_spinor<SP>(src, pv, nb1, v);
         mdv_sub(u, v, acc);
-        ld_link<P>(lng_q, pv, dir, nb3, lng.scale, u);
-        ld_spinor<P>(src, pv, nb3, v);
+        ld_link<LP>(lng_q, pv, dir, nb3, lng.scale, u);
+        ld_spinor<SP>(src, pv, nb3, v);
         mdv_sub(u, v, acc);
+    }
+}
+
+template <int P>
+__device__ __forceinline__ void dslash_site(const Geom &g, int pv, const LinkSet &fat, const LinkSet &lng,
+                                            const void *src, int p, int i, typename Acc<P>::T acc[6])
+{
+    dslash_site2<P, P>(g, pv, fat, lng, src, p, i, acc);
+}
+
+// Multi-RHS form: the links of site i are loaded once and applied to R right-hand sides whose fields are
+// src0 + sys[r] * stride (sys[r] < 0: slot unused).  acc[r] receives (D src_r)(i).
+template <int LP, int SP, int R>
+__device__ __forceinline__ void dslash_site_mrhs(const Geom &g, int pv, const LinkSet &fat, const LinkSet &lng,
+                                                 const char *src0, size_t stride, const int sys[R], int p, int i,
+                                                 typename Acc2<LP, SP>::T acc[R][6])
+{
+    using T = typename Acc2<LP, SP>::T;
+    const SiteCoord c = site_coord(g, i, p);
+    const void *fat_p = p ? fat.par[1] : fat.par[0], *fat_q = p ? fat.par[0] : fat.par[1];
+    const void *lng_p = p ? lng.par[1] : lng.par[0], *lng_q = p ? lng.par[0] : lng.par[1];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) acc[r][k] = T(0);
+#pragma unroll
+    for (int dir = 0; dir < 4; ++dir) {
+        const int nf1 = nbr_index(g, c, i, dir, 1);
+        const int nf3 = nbr_index(g, c, i, dir, 3);
+        const int nb1 = nbr_index(g, c, i, dir, -1);
+        const int nb3 = nbr_index(g, c, i, dir, -3);
+        T u[18], v[6];
+        ld_link<LP>(fat_p, pv, dir, i, fat.scale, u);
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (sys[r] >= 0) {
+                ld_spinor<SP>(src0 + sys[r] * stride, pv, nf1, v);
+                mv_add(u, v, acc[r]);
+            }
+        ld_link<LP>(lng_p, pv, dir, i, lng.scale, u);
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (sys[r] >= 0) {
+                ld_spinor<SP>(src0 + sys[r] * stride, pv, nf3, v);
+                mv_add(u, v, acc[r]);
+            }
+        ld_link<LP>(fat_q, pv, dir, nb1, fat.scale, u);
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (sys[r] >= 0) {
+                ld_spinor<SP>(src0 + sys[r] * stride, pv, nb1, v);
+                mdv_sub(u, v, acc[r]);
+            }
+        ld_link<LP>(lng_q, pv, dir, nb3, lng.scale, u);
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (sys[r] >= 0) {
+                ld_spinor<SP>(src0 + sys[r] * stride, pv, nb3, v);
+                mdv_sub(u, v, acc[r]);
+            }
     }
 }
 

@@ -314,7 +314,8 @@ KQ_API KuQCDStatus kq_kuqcd_solve_multishift(void **hp_x, void *hp_b, KuQCDInver
         // optional sloppy solver for FP64 links: KUQCD_SOLVER=mixed, target |r_k| < sqrt(tol) (the reference's
         // stopping rule zeta_k^2 |r|^2 < tol bounds the squared residual norm of shift k)
         const char *solver = getenv("KUQCD_SOLVER");
-        const bool mixed = dbl && solver && strcmp(solver, "mixed") == 0;
+        const bool mixed_half = dbl && solver && strcmp(solver, "mixed-half") == 0;
+        const bool mixed = mixed_half || (dbl && solver && strcmp(solver, "mixed") == 0);
         const size_t vh = (size_t)S.lat[0] * S.lat[1] * S.lat[2] * S.lat[3] / 2;
         const size_t esz = dbl ? 8 : 4;
         const void *b = hp_b;
@@ -339,7 +340,7 @@ KQ_API KuQCDStatus kq_kuqcd_solve_multishift(void **hp_x, void *hp_b, KuQCDInver
             const double *bd = static_cast<const double *>(b);
             for (size_t e = 0; e < vh * 6; ++e) bb += bd[e] * bd[e];
             sp.solver = KQ_SOLVER_MIXED;
-            sp.prec = KUQCD_SINGLE;
+            sp.prec = mixed_half ? KUQCD_HALF : KUQCD_SINGLE;
             sp.rel_residual = bb > 0 ? std::sqrt(param->tol / bb) : 1e-10;
         }
         kq_solve_info info;

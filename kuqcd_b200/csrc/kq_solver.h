@@ -43,10 +43,12 @@ struct CgmResult {
     int status;
     double rnorm2;
     double zeta[kMaxShift];
+    long long launches;  // kernels enqueued (graph nodes included)
 };
 
-// Plain multishift CG, every vector in `prec` (FP64 or FP32), scalars and reductions in FP64.
-cudaError_t cgm_solve(const Geom &g, const GaugeDev &gd, int prec, const CgmBuffers &w, int parity, int ns,
+// Multishift CG with the reference's recurrences: vectors in `prec` (FP64 or FP32), links in `lp` (= prec, or
+// HALF links with FP32 vectors), scalars and reductions in FP64.
+cudaError_t cgm_solve(const Geom &g, const GaugeDev &gd, int lp, int prec, const CgmBuffers &w, int parity, int ns,
                       const double *shifts, double tol, int max_iter, int chunk, CgmResult *res, cudaStream_t s);
 
 }  // namespace kq

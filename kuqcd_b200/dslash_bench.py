@@ -1,0 +1,65 @@
+"""Stand-alone HISQ dslash driver: applies the even-odd dslash `--reps` times on synthetic fields and prints the
+achieved rate (1146 flop per output site; compulsory bytes 2400 / 1200 / 608 per site for DOUBLE / SINGLE /
+HALF).  Used for profiling the dslash kernels in isolation.
+
+    python -m kuqcd_b200.dslash_bench --dims 32 32 32 32 --prec double --reps 20
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+import numpy as np
+import torch
+
+import kuqcd_b200 as K
+
+PRECS = {"double": K.KUQCD_DOUBLE, "single": K.KUQCD_SINGLE, "half": K.KUQCD_HALF}
+BYTES = {K.KUQCD_DOUBLE: 2400, K.KUQCD_SINGLE: 1200, K.KUQCD_HALF: 608}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--dims", type=int, nargs=4, default=[32, 32, 32, 32])
+    ap.add_argument("--prec", choices=list(PRECS), nargs="+", default=["double"])
+    ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--eps", type=float, default=0.3)
+    args = ap.parse_args()
+    dims = tuple(args.dims)
+    V = int(np.prod(dims))
+    Vh = V // 2
+    ctx = K.Context(dims)
+    dfat = torch.empty(V * 72, dtype=torch.float64, device="cuda")
+    dlng = torch.empty(V * 72, dtype=torch.float64, device="cuda")
+    ctx.make_links(args.eps, 1, dfat, dlng)
+    ctx.load_links(K.KUQCD_FAT_LINK, dfat.cpu().numpy())
+    ctx.load_links(K.KUQCD_LONG_LINK, dlng.cpu().numpy())
+    del dfat, dlng
+    db = torch.empty(Vh * 6, dtype=torch.float64, device="cuda")
+    ctx.make_source(1, 2, db)
+    hb = db.cpu().numpy()
+    stream = torch.cuda.Stream()
+    out = {}
+    for name in args.prec:
+        prec = PRECS[name]
+        ctx.prepare(prec)
+        a = torch.zeros(ctx.spinor_bytes(prec), dtype=torch.uint8, device="cuda")
+        o = torch.zeros_like(a)
+        ctx.upload(prec, hb, a)
+        for _ in range(args.warmup):
+            ctx.dslash(prec, a, o, 0, stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for r in range(args.reps):
+            src, dst = (a, o) if r % 2 == 0 else (o, a)
+            ctx.dslash(prec, src, dst, r % 2, stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / args.reps * 1e-3
+        out[name] = {"us": t * 1e6, "gflops": 1146 * Vh / t / 1e9, "gbs": BYTES[prec] * Vh / t / 1e9}
+    print(json.dumps({"dims": list(dims), "dslash": out}))
+
+
+if __name__ == "__main__":
+    main()

@@ -53,7 +53,8 @@ class SolveParam(C.Structure):
 
 class SolveInfo(C.Structure):
     _fields_ = [("iter", C.c_int), ("iter_refine", C.c_int), ("status", C.c_int), ("num_shift", C.c_int),
-                ("true_residual", C.c_double * 64), ("seconds", C.c_double)]
+                ("true_residual", C.c_double * 64), ("seconds", C.c_double), ("kernel_launches", C.c_longlong),
+                ("sloppy_residual", C.c_double)]
 
 
 # every symbol include/*.h declares for the C ABI (checked by the CPU test suite)

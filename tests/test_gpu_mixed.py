@@ -1,0 +1,81 @@
+"""GPU tests of the mixed-precision multishift solver (sloppy multishift + batched reliable-update refinement):
+every shift's FP64 true relative residual, recomputed by the oracle on the CPU, meets the target."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import kuqcd_b200 as K
+from oracle import oracle as O
+from tests.test_gpu_cgm import api_solve
+
+
+def ctx_for(dims, eps, seed):
+    fat, lng = O.make_links(dims, eps, seed)
+    ctx = K.Context(dims)
+    ctx.load_links(K.KUQCD_FAT_LINK, fat)
+    ctx.load_links(K.KUQCD_LONG_LINK, lng)
+    return ctx, fat, lng
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sloppy", [K.KUQCD_SINGLE, K.KUQCD_HALF])
+@pytest.mark.parametrize("parity", [0, 1])
+def test_mixed_8x4_config_reaches_1e10(cuda, sloppy, parity):
+    dims = (8, 8, 8, 8)
+    ctx, fat, lng = ctx_for(dims, 0.3, 1234)
+    b = O.make_source(dims, parity, 99)
+    sig = list(0.05 ** 2 + np.logspace(-4, 0, 12))
+    xs, info = ctx.solve(b, sig, parity=parity, solver=K.KQ_SOLVER_MIXED, prec=sloppy, rel_residual=1e-10)
+    assert info.status == 0
+    assert info.iter > 0 and info.iter_refine > 0
+    for k, s in enumerate(sig):
+        r = O.true_residual(dims, fat, lng, parity, s, b, xs[k])
+        assert r <= 1.2e-10, (k, r)
+        # the device's own FP64 residual agrees with the oracle's
+        assert abs(info.true_residual[k] - r) <= 0.05 * r + 1e-13
+    ctx.close()
+
+
+@pytest.mark.gpu
+def test_mixed_single_shift_and_tight_target(cuda):
+    dims = (8, 4, 4, 8)
+    ctx, fat, lng = ctx_for(dims, 0.4, 5)
+    b = O.make_source(dims, 0, 5)
+    xs, info = ctx.solve(b, [0.002], solver=K.KQ_SOLVER_MIXED, prec=K.KUQCD_SINGLE, rel_residual=1e-12)
+    assert info.status == 0
+    assert O.true_residual(dims, fat, lng, 0, 0.002, b, xs[0]) <= 1.2e-12
+    ctx.close()
+
+
+@pytest.mark.gpu
+def test_mixed_matches_plain_solution(cuda):
+    dims = (8, 8, 4, 4)
+    ctx, fat, lng = ctx_for(dims, 0.3, 77)
+    b = O.make_source(dims, 0, 7)
+    sig = [0.01, 0.1, 1.0]
+    xm, im = ctx.solve(b, sig, solver=K.KQ_SOLVER_MIXED, prec=K.KUQCD_HALF, rel_residual=1e-11)
+    xp, ip = ctx.solve(b, sig, solver=K.KQ_SOLVER_CGM, prec=K.KUQCD_DOUBLE, tol=(1e-12) ** 2 * float(b @ b))
+    for k in range(3):
+        # both solve (sigma + D^dag D) x = b; the difference is bounded by the residuals over sigma
+        bound = 2e-11 * np.linalg.norm(b) / sig[k]
+        assert np.linalg.norm(xm[k] - xp[k]) <= bound
+    ctx.close()
+
+
+@pytest.mark.gpu
+def test_mixed_through_reference_api(cuda, monkeypatch):
+    """KUQCD_SOLVER=mixed switches kuqcd_solve_multishift (DOUBLE links) to the mixed solver; the reference's
+    stopping rule zeta_k^2 |r|^2 < tol becomes the true residual bound |r_k| < sqrt(tol)."""
+    monkeypatch.setenv("KUQCD_SOLVER", "mixed")
+    dims = (8, 8, 8, 8)
+    fat, lng = O.make_links(dims, 0.3, 4321)
+    b = O.make_source(dims, 0, 11)
+    m, sig = 0.05, np.logspace(-4, 0, 12)
+    ab = m * m + sig
+    refsh = [ab[0]] + list(sig[1:] - sig[0])
+    tol = (1e-10) ** 2 * float(b @ b)
+    st, xs, it = api_solve(dims, fat, lng, b, refsh, tol, 10000)
+    assert st == 0 and it > 0
+    for k in range(12):
+        assert O.true_residual(dims, fat, lng, 0, ab[k], b, xs[k]) <= 1.2e-10
