@@ -228,6 +228,7 @@ def run_ours(args):
     # ---------------- dslash roofline: the solver's dominant kernel, CUDA events on the launching stream
     dsl = {}
     # a dedicated (non-default) torch stream: the kernels run where the events are recorded
+    stream = torch.cuda.Stream()
     for name, prec in [("fp64", K.KUQCD_DOUBLE), ("fp32", K.KUQCD_SINGLE), ("half", K.KUQCD_HALF)]:
         nbp = ctx.spinor_bytes(prec)
         a = torch.zeros(nbp, dtype=torch.uint8, device="cuda")
