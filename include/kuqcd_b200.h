@@ -71,6 +71,15 @@ KuQCDStatus kq_dslash(kq_context *ctx, int prec, const void *d_src, void *d_dst,
  * Replaces DiracHISQ::MdaggM (dirac_hisq.cpp:457-462) followed by Axmy (spinor_field.cpp:130-144). */
 KuQCDStatus kq_mdagm(kq_context *ctx, int prec, double sigma, const void *d_src, void *d_dst, void *d_tmp,
                      int parity, void *stream);
+/* kq_mdagm without a caller temporary and without any device allocation (no counterpart in the reference).
+ * For callers that cannot allocate while they apply the operator: work being recorded into a CUDA graph, where
+ * cudaMalloc is not allowed during capture, or applications whose own pool owns nearly all device memory.  The
+ * temporary comes from a 32 MiB array that each GPU loading the library holds until exit; larger fields are
+ * rejected with KUQCD_ERR_INVALID_PARAM.  All calls share that array: calls overlapping on the GPU race.  Links
+ * must already be resident in prec.  The first call on a device looks up the array's address; make it before any
+ * stream capture. */
+KuQCDStatus kq_mdagm_noalloc(kq_context *ctx, int prec, double sigma, const void *d_src, void *d_dst, int parity,
+                             void *stream);
 
 /* ---------------------------------------------------------------- solver */
 enum {

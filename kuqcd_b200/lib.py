@@ -62,6 +62,7 @@ EXPORTED_SYMBOLS = [
     "kq_kuqcd_init", "kq_kuqcd_load_gaugefield", "kq_kuqcd_solve_multishift", "kq_kuqcd_gauge_free",
     "kq_kuqcd_end", "kq_context_create", "kq_context_destroy", "kq_load_links", "kq_prepare_links",
     "kq_spinor_bytes", "kq_spinor_upload", "kq_spinor_download", "kq_spinor_convert", "kq_dslash", "kq_mdagm",
+    "kq_mdagm_noalloc",
     "kq_solve_multishift", "kq_solve_multishift_device", "kq_true_residuals", "kq_make_links_record",
     "kq_make_source_record", "kq_last_error",
 ]
@@ -103,6 +104,7 @@ def library() -> C.CDLL:
         "kq_spinor_convert": (i, [vp, vp, i, vp, i, vp]),
         "kq_dslash": (i, [vp, i, vp, vp, i, vp]),
         "kq_mdagm": (i, [vp, i, d, vp, vp, vp, i, vp]),
+        "kq_mdagm_noalloc": (i, [vp, i, d, vp, vp, i, vp]),
         "kq_solve_multishift": (i, [vp, C.POINTER(SolveParam), vp, C.POINTER(vp), C.POINTER(SolveInfo)]),
         "kq_solve_multishift_device": (i, [vp, C.POINTER(SolveParam), vp, vp, C.POINTER(SolveInfo)]),
         "kq_true_residuals": (i, [vp, i, i, C.POINTER(d), vp, vp, C.POINTER(d)]),
@@ -222,6 +224,10 @@ class Context:
     def mdagm(self, prec: int, sigma: float, src, dst, tmp, parity: int, stream=None):
         self._chk(library().kq_mdagm(self._h, prec, sigma, _ptr(src), _ptr(dst), _ptr(tmp), parity, stream),
                   "kq_mdagm")
+
+    def mdagm_noalloc(self, prec: int, sigma: float, src, dst, parity: int, stream=None) -> int:
+        """kq_mdagm_noalloc: returns the status (callers test the rejection paths)."""
+        return library().kq_mdagm_noalloc(self._h, prec, sigma, _ptr(src), _ptr(dst), parity, stream)
 
     @staticmethod
     def _param(shifts, parity, solver, prec, host_prec, max_iter, tol, rel_residual, shift_mode):
