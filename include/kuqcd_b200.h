@@ -84,7 +84,11 @@ KuQCDStatus kq_mdagm_noalloc(kq_context *ctx, int prec, double sigma, const void
 /* ---------------------------------------------------------------- solver */
 enum {
     KQ_SOLVER_CGM = 0,        /* multishift CG with the reference's recurrences (CGM::Invert), FP64 or FP32 */
-    KQ_SOLVER_MIXED = 1       /* sloppy multishift + per-shift reliable-update refinement to an FP64 target */
+    KQ_SOLVER_MIXED = 1,      /* relaxed-precision multishift (FP64 -> FP32 -> HALF operator as |r| falls) with an
+                                 FP64 true-residual check and batched reliable-update refinement of any shift left
+                                 above rel_residual; prec = SINGLE or HALF is the cheapest operator it may use */
+    KQ_SOLVER_CGM_WINDOWED = 2 /* the CGM recurrences in FP64 with windowed shift updates (same iterates as
+                                  KQ_SOLVER_CGM up to rounding, 4N -> (4N+8)/8 vector sweeps per iteration) */
 };
 
 typedef struct {

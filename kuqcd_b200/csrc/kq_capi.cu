@@ -10,6 +10,7 @@
 
 #include "kq_context.h"
 #include "kq_internal.h"
+#include "kq_msrelax.h"
 #include "kq_prec.cuh"
 #include "kq_solver.h"
 
@@ -394,6 +395,25 @@ KQ_API KuQCDStatus kq_solve_multishift_device(kq_context *ctx, const kq_solve_pa
     cudaError_t e = cudaSuccess;
     if (p->solver == KQ_SOLVER_MIXED) {
         e = mixed_solve(ctx, p, sig, d_b, d_x, info);
+    } else if (p->solver == KQ_SOLVER_CGM_WINDOWED) {
+        MsBuffers w;
+        Carve probe(nullptr);
+        ms_layout(probe, ctx->g, p->num_shift, d_b, d_x, w);
+        e = ensure_work(ctx, probe.off);
+        if (e == cudaSuccess) {
+            Carve c(ctx->work);
+            ms_layout(c, ctx->g, p->num_shift, d_b, d_x, w);
+            double rs[kMaxShift];
+            rs[0] = sig[0];
+            for (int k = 1; k < p->num_shift; ++k) rs[k] = sig[k] - sig[0];
+            MsResult r;
+            e = ms_solve(ctx, w, p->parity, p->num_shift, rs, p->tol, p->max_iter, 0.0, 0.0, &r);
+            if (e == cudaSuccess) {
+                info->iter = r.iter;
+                info->status = r.status;
+                info->kernel_launches = r.launches;
+            }
+        }
     } else {
         const int prec = prec_from_api(p->prec);
         if (prec != P64 && prec != P32) {

@@ -132,6 +132,48 @@ __device__ __forceinline__ void dslash_site(const Geom &g, int pv, const LinkSet
     dslash_site2<P, P>(g, pv, fat, lng, src, p, i, acc);
 }
 
+// General form: links in LP, input spinors stored in SP, arithmetic in T (double only for FP64 links).
+// Used where a sloppy operator reads an FP64 vector (the inexact-matvec phases of the multishift solver).
+template <int LP, int SP, typename T>
+__device__ __forceinline__ void dslash_site_t(const Geom &g, int pv, const LinkSet &fat, const LinkSet &lng,
+                                              const void *src, int p, int i, T acc[6])
+{
+    const SiteCoord c = site_coord(g, i, p);
+    const void *fat_p = p ? fat.par[1] : fat.par[0], *fat_q = p ? fat.par[0] : fat.par[1];
+    const void *lng_p = p ? lng.par[1] : lng.par[0], *lng_q = p ? lng.par[0] : lng.par[1];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) acc[k] = T(0);
+#pragma unroll
+    for (int dir = 0; dir < 4; ++dir) {
+        const int nf1 = nbr_index(g, c, i, dir, 1);
+        const int nf3 = nbr_index(g, c, i, dir, 3);
+        const int nb1 = nbr_index(g, c, i, dir, -1);
+        const int nb3 = nbr_index(g, c, i, dir, -3);
+        typename Acc<LP>::T ul[18];
+        T u[18], v[6];
+        ld_link<LP>(fat_p, pv, dir, i, fat.scale, ul);
+#pragma unroll
+        for (int k = 0; k < 18; ++k) u[k] = (T)ul[k];
+        ld_spinor_as<SP>(src, pv, nf1, v);
+        mv_add(u, v, acc);
+        ld_link<LP>(lng_p, pv, dir, i, lng.scale, ul);
+#pragma unroll
+        for (int k = 0; k < 18; ++k) u[k] = (T)ul[k];
+        ld_spinor_as<SP>(src, pv, nf3, v);
+        mv_add(u, v, acc);
+        ld_link<LP>(fat_q, pv, dir, nb1, fat.scale, ul);
+#pragma unroll
+        for (int k = 0; k < 18; ++k) u[k] = (T)ul[k];
+        ld_spinor_as<SP>(src, pv, nb1, v);
+        mdv_sub(u, v, acc);
+        ld_link<LP>(lng_q, pv, dir, nb3, lng.scale, ul);
+#pragma unroll
+        for (int k = 0; k < 18; ++k) u[k] = (T)ul[k];
+        ld_spinor_as<SP>(src, pv, nb3, v);
+        mdv_sub(u, v, acc);
+    }
+}
+
 // Multi-RHS form: the links of site i are loaded once and applied to R right-hand sides whose fields are
 // src0 + sys[r] * stride (sys[r] < 0: slot unused).  acc[r] receives (D src_r)(i).
 template <int LP, int SP, int R>

@@ -1,8 +1,10 @@
 // Mixed-precision multishift solver (KQ_SOLVER_MIXED): every shift reaches an FP64 true relative residual target.
 //
-// Phase 1  sloppy multishift CG (the CGM recurrences of inverter_cgm.cpp:17-87) with FP32 vectors and FP32 or HALF
-//          links, stopped per shift at a loose tolerance delta1 (the sloppy operator's attainable accuracy).
-// Phase 2  all shifted systems (sigma_k + D^dag D) x_k = b refined together by a multi-RHS CG with reliable updates:
+// Phase 1  relaxed-precision multishift CG (kq_msrelax.cu: the CGM recurrences of inverter_cgm.cpp:17-87 with FP64
+//          vectors, the operator switched to FP32 and then HALF links as the residual falls below the points where
+//          their accumulated error still fits under the target), stopped at a fraction of the target.
+// Phase 2  an FP64 check of every shift's true residual; shifts above the target (rare: the operator-error
+//          model missed) are refined together by a multi-RHS CG with reliable updates:
 //          FP32 / HALF-link iterations in lockstep over the still-active systems, each dslash loading every link
 //          once for R systems; when a system's iterated residual has fallen by `delta` since its last true residual
 //          (or below the target), its FP32 correction is folded into the FP64 solution and its residual is
@@ -19,6 +21,7 @@
 
 #include "kq_context.h"
 #include "kq_dslash_core.cuh"
+#include "kq_msrelax.h"
 
 namespace kq {
 
@@ -421,10 +424,14 @@ cudaError_t mixed_solve(::kq_context *ctx, const kq_solve_param *param, const do
         return cudaErrorInvalidValue;
     }
     const double target = param->rel_residual > 0 ? param->rel_residual : 1e-10;
-    // phase-1 stopping point: about the attainable accuracy of the sloppy operator
-    const double delta1 = env_double("KUQCD_MIXED_DELTA1", lp == P32 ? 1e-5 : 1e-4);
-    const double delta = env_double("KUQCD_MIXED_DELTA", 0.1);
-    const int need[2] = {P64, lp};
+    // Effective error of the sloppy operators relative to |r| at the switch (measured on the oracle: the FP32
+    // operator's residual gap grows to ~1e-5 x, the HALF one to ~1e-3 x the residual norm at which it starts).
+    const double eps32 = env_double("KUQCD_RELAX_EPS32", 1e-5);
+    const double eps16 = env_double("KUQCD_RELAX_EPS16", 1e-3);
+    const double relax_frac = env_double("KUQCD_RELAX_FRAC", 0.3);  // share of the target each precision may use
+    const double stop_frac = env_double("KUQCD_RELAX_STOP", 0.7);   // recursive-residual stop, x target
+    const double delta = env_double("KUQCD_MIXED_DELTA", 0.1);     // reliable-update trigger of the refinement
+    const int need[3] = {P64, P32, lp};  // the relaxed schedule runs FP64, then FP32, then (HALF) links
     for (int p : need)
         if (!ctx->gd.have[p]) {
             if (kq_prepare_links(ctx, p == P64 ? KUQCD_DOUBLE : p == P32 ? KUQCD_SINGLE : KUQCD_HALF) != KUQCD_SUCCESS)
@@ -433,16 +440,9 @@ cudaError_t mixed_solve(::kq_context *ctx, const kq_solve_param *param, const do
     const size_t vb32 = spinor_bytes(g, P32), vb64 = spinor_bytes(g, P64);
     const int sb = (g.vh + kBS - 1) / kBS;
     // ---- workspace
-    auto layout = [&](Carve &c, CgmBuffers &cw, MrBuffers &mw) {
-        cw.vec_bytes = vb32;
-        cw.b = c.take(vb32);
-        cw.r = c.take(vb32);
-        cw.s = c.take(vb32);
-        cw.tmp = c.take(vb32);
-        cw.p = c.take(vb32 * ns);
-        cw.x = c.take(vb32 * ns);
-        cw.partials = static_cast<double *>(c.take(sizeof(double) * (size_t)sb * ns));
-        cw.state = static_cast<CgmState *>(c.take(sizeof(CgmState)));
+    auto layout = [&](Carve &c, MsBuffers &cw, MrBuffers &mw) {
+        ms_layout(c, g, ns, d_b, d_x, cw);
+        mw.partials = static_cast<double *>(c.take(sizeof(double) * (size_t)sb * ns));
         mw.b = d_b;
         mw.x64 = d_x;
         mw.vb32 = vb32;
@@ -454,25 +454,23 @@ cudaError_t mixed_solve(::kq_context *ctx, const kq_solve_param *param, const do
         mw.ap = c.take(vb32 * ns);
         mw.tmp = c.take(vb32 * ns);
         mw.tmp64 = c.take(vb64 * ns);
-        mw.partials = cw.partials;
         mw.st = static_cast<MrState *>(c.take(sizeof(MrState)));
     };
-    CgmBuffers cw;
+    MsBuffers cw;
     MrBuffers mw;
     Carve probe(nullptr);
     layout(probe, cw, mw);
     KQ_CUDA_TRY(ensure_work(ctx, probe.off));
     Carve c(ctx->work);
     layout(c, cw, mw);
-    cw.poll = ctx->poll;
     long long launches = 0;
 
     // ---- |b|^2
     {
         const int pv = pad_sites(g.vh);
-        norm2_partials_kernel<<<sb, kBS, 0, s>>>(g.vh, pv, d_b, cw.partials);
+        norm2_partials_kernel<<<sb, kBS, 0, s>>>(g.vh, pv, d_b, mw.partials);
         std::vector<double> h(sb);
-        KQ_CUDA_TRY(cudaMemcpyAsync(h.data(), cw.partials, sizeof(double) * sb, cudaMemcpyDeviceToHost, s));
+        KQ_CUDA_TRY(cudaMemcpyAsync(h.data(), mw.partials, sizeof(double) * sb, cudaMemcpyDeviceToHost, s));
         KQ_CUDA_TRY(cudaStreamSynchronize(s));
         launches += 1;
         double bb = 0;
@@ -498,20 +496,18 @@ cudaError_t mixed_solve(::kq_context *ctx, const kq_solve_param *param, const do
             hs.rr[k] = 1.0;
         }
         KQ_CUDA_TRY(cudaMemcpyAsync(mw.st, &hs, sizeof(hs), cudaMemcpyHostToDevice, s));
-        // phase 1 tolerance in the reference's stopping rule: zeta_k^2 |r|^2 < (delta1 |b|)^2
-        KQ_CUDA_TRY(spinor_convert(g, d_b, P64, const_cast<void *>(cw.b), P32, s));
+        // phase 1: relaxed-precision multishift, stopped (reference rule) at a fraction of the target so that the
+        // operator's accumulated error still fits under it
         double rs[kMaxShift];
         rs[0] = sig[0];
         for (int k = 1; k < ns; ++k) rs[k] = sig[k] - sig[0];
-        CgmResult r1;
-        KQ_CUDA_TRY(cgm_solve(g, ctx->gd, lp, P32, cw, param->parity, ns, rs, delta1 * delta1 * bb,
-                              param->max_iter > 0 ? param->max_iter : 100000, 8, &r1, s));
+        const double rho32 = relax_frac * target / eps32;
+        const double rho16 = lp == P16 ? relax_frac * target / eps16 : 0.0;
+        MsResult r1;
+        KQ_CUDA_TRY(ms_solve(ctx, cw, param->parity, ns, rs, stop_frac * stop_frac * target * target * bb,
+                             param->max_iter > 0 ? param->max_iter : 100000, rho32, rho16, &r1));
         info->iter = r1.iter;
-        launches += r1.launches + 1;
-        for (int k = 0; k < ns; ++k)
-            KQ_CUDA_TRY(spinor_convert(g, static_cast<char *>(cw.x) + k * vb32, P32,
-                                       static_cast<char *>(d_x) + k * vb64, P64, s));
-        launches += ns;
+        launches += r1.launches;
     }
 
     // ---- phase 2

@@ -86,6 +86,24 @@ template <> __device__ __forceinline__ void st_spinor<2>(void *base, int pv, int
     static_cast<int4 *>(base)[i] = w;
 }
 
+// load / store a spinor of storage precision P into / from registers of any floating type T
+template <int P, typename T>
+__device__ __forceinline__ void ld_spinor_as(const void *base, int pv, int i, T v[6])
+{
+    typename Acc<P>::T w[6];
+    ld_spinor<P>(base, pv, i, w);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) v[k] = (T)w[k];
+}
+template <int P, typename T>
+__device__ __forceinline__ void st_spinor_as(void *base, int pv, int i, const T v[6])
+{
+    typename Acc<P>::T w[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) w[k] = (typename Acc<P>::T)v[k];
+    st_spinor<P>(base, pv, i, w);
+}
+
 // ------------------------------------------------------------------------------------------------ links
 // One 3x3 complex matrix, row-major u[2*(col + 3*row)] (re, im).
 // FP64: 9 double2 planes per direction.     dir stride = 9 * pv double2

@@ -31,7 +31,7 @@ KUQCD_WILSON_LINK, KUQCD_FAT_LINK, KUQCD_LONG_LINK = 0, 1, 2
 KUQCD_GAUGE_RECON_NO, KUQCD_GAUGE_RECON_U14, KUQCD_GAUGE_RECON_12, KUQCD_GAUGE_RECON_8 = 18, 14, 12, 8
 KUQCD_WILSON_DIRAC, KUQCD_WILSONPC_DIRAC, KUQCD_HISQ_DIRAC, KUQCD_HISQPC_DIRAC = 0, 1, 2, 3
 KUQCD_CG, KUQCD_CGM = 0, 1
-KQ_SOLVER_CGM, KQ_SOLVER_MIXED = 0, 1
+KQ_SOLVER_CGM, KQ_SOLVER_MIXED, KQ_SOLVER_CGM_WINDOWED = 0, 1, 2
 
 
 class KuQCDGaugeParam(C.Structure):

