@@ -33,18 +33,34 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "HISQ dslash GFLOP/s + HBM GB/s; multishift CG time to 1e-10, mixed vs plain FP64"
-DIMS = (32, 32, 32, 32)
-EPS, MASS, NSHIFT = 0.3, 0.05, 12
 REL_RES = 1e-10
 DSLASH_FLOPS = 1146          # per output site
 DSLASH_BYTES = {8: 2400, 4: 1200, 2: 608}   # compulsory bytes per output site: 16 links + 1 in + 1 out spinor
-# Iterations the reference CGM (inverter_cgm.cpp:17-87) needs on this workload (seed 1000, tol (1e-10)^2 |b|^2,
-# reference-semantics shifts), measured by running oracle/ref_iterations.py to convergence.
-REF_ITERS_32 = 295
+# Workloads.  "32": 32^4, eps 0.3, m 0.05, 12 shifts 1e-4..1 (the default).  "48": 48^3x96, eps 0.4, m 0.02,
+# 16 shifts 1e-5..1.  ref_iters: iterations the reference CGM (inverter_cgm.cpp:17-87) needs on the workload
+# (seed 1000, tol (1e-10)^2 |b|^2, reference-semantics shifts): for 32^4 counted by running oracle/ref_iterations.py
+# to convergence; for 48^3x96 (hours on a CPU) the count of the GPU solver that reproduces the reference's
+# recurrences in kernel order (KQ_SOLVER_CGM, same count as the reference on every tested lattice).
+CONFIGS = {
+    "32": dict(dims=(32, 32, 32, 32), eps=0.3, mass=0.05, nshift=12, smin=1e-4, ref_iters=295),
+    "48": dict(dims=(48, 48, 48, 96), eps=0.4, mass=0.02, nshift=16, smin=1e-5, ref_iters=None),
+}
+DIMS, EPS, MASS, NSHIFT, SMIN, REF_ITERS = (32, 32, 32, 32), 0.3, 0.05, 12, 1e-4, 295
+
+
+def select_config(name):
+    global DIMS, EPS, MASS, NSHIFT, SMIN, REF_ITERS
+    c = CONFIGS[name]
+    DIMS, EPS, MASS, NSHIFT, SMIN, REF_ITERS = c["dims"], c["eps"], c["mass"], c["nshift"], c["smin"], c["ref_iters"]
 
 
 def shifts_abs():
-    return list(MASS * MASS + np.logspace(-4, 0, NSHIFT))
+    return list(MASS * MASS + np.logspace(np.log10(SMIN), 0, NSHIFT))
+
+
+def workload_name(dims):
+    return (f"multishift CG {'x'.join(map(str, dims))}, {NSHIFT} shifts {SMIN:g}..1, m={MASS}, eps={EPS}, "
+            f"per-shift true residual {REL_RES}")
 
 
 def dist_env():
@@ -191,42 +207,6 @@ def run_ours(args):
     ms_step, iters, true_res = main_run["ms"], [main_run["iters"]], [main_run["true_res"]]
     wall_s = main_run["wall_ms"] * 1e-3 * args.steps
 
-    # ---------------- e2e: reference-facing call with pinned host buffers
-    hb_pin = torch.from_numpy(hb).pin_memory()
-    hx_pin = [torch.empty(Vh * 6, dtype=torch.float64).pin_memory() for _ in range(NSHIFT)]
-    os.environ["KUQCD_SOLVER"] = args.solver
-    K.kuqcd_gauge_free()
-    K.kuqcd_init()
-    gp = K.KuQCDGaugeParam()
-    gp.lat[:] = dims
-    gp.halo_depth, gp.od, gp.site_subset = 0, K.KUQCD_TZYX_ORDER, K.KUQCD_ALL
-    gp.gauge_order, gp.prec, gp.recon = K.KUQCD_NORMAL_ORDER, K.KUQCD_DOUBLE, K.KUQCD_GAUGE_RECON_NO
-    gp.link_type = K.KUQCD_FAT_LINK
-    assert K.kuqcd_load_gaugefield(hfat, gp) == 0
-    gp.link_type = K.KUQCD_LONG_LINK
-    assert K.kuqcd_load_gaugefield(hlng, gp) == 0
-    refsh = [sig[0]] + [s - sig[0] for s in sig[1:]]
-    shc = (C.c_double * NSHIFT)(*refsh)
-    ip = K.KuQCDInvertParam(dslash_type=K.KUQCD_HISQPC_DIRAC, inverter_type=K.KUQCD_CGM,
-                            matpc_type=K.KUQCD_EVEN_EVEN, prec=K.KUQCD_DOUBLE, num_shift=NSHIFT, max_iter=100000,
-                            iter=0, tol=(REL_RES ** 2) * bnorm2, shifts=C.cast(shc, C.POINTER(C.c_double)))
-    xs_np = [x.numpy() for x in hx_pin]
-    b_np = hb_pin.numpy()
-    for _ in range(max(1, args.warmup)):
-        assert K.kuqcd_solve_multishift(xs_np, b_np, ip) == 0
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        assert K.kuqcd_solve_multishift(xs_np, b_np, ip) == 0
-    e2e_s = (time.perf_counter() - t0) / args.steps
-    K.kuqcd_gauge_free()
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-
     # ---------------- dslash roofline: the solver's dominant kernel, CUDA events on the launching stream
     dsl = {}
     # a dedicated (non-default) torch stream: the kernels run where the events are recorded
@@ -248,6 +228,45 @@ def run_ours(args):
         t_launch = s0.elapsed_time(s1) / reps * 1e-3
         dsl[name] = {"ms": t_launch * 1e3, "gflops": DSLASH_FLOPS * Vh / t_launch / 1e9,
                      "gbs": DSLASH_BYTES[prec] * Vh / t_launch / 1e9}
+    ctx.close()  # free its links and workspace before the API path loads its own copy
+
+    # ---------------- e2e: reference-facing call with pinned host buffers
+    hb_pin = torch.from_numpy(hb).pin_memory()
+    hx_pin = [torch.empty(Vh * 6, dtype=torch.float64).pin_memory() for _ in range(NSHIFT)]
+    os.environ["KUQCD_SOLVER"] = args.solver
+    K.kuqcd_gauge_free()
+    K.kuqcd_init()
+    gp = K.KuQCDGaugeParam()
+    gp.lat[:] = dims
+    gp.halo_depth, gp.od, gp.site_subset = 0, K.KUQCD_TZYX_ORDER, K.KUQCD_ALL
+    gp.gauge_order, gp.prec, gp.recon = K.KUQCD_NORMAL_ORDER, K.KUQCD_DOUBLE, K.KUQCD_GAUGE_RECON_NO
+    gp.link_type = K.KUQCD_FAT_LINK
+    assert K.kuqcd_load_gaugefield(hfat, gp) == 0
+    gp.link_type = K.KUQCD_LONG_LINK
+    assert K.kuqcd_load_gaugefield(hlng, gp) == 0
+    refsh = [sig[0]] + [s - sig[0] for s in sig[1:]]
+    shc = (C.c_double * NSHIFT)(*refsh)
+    ip = K.KuQCDInvertParam(dslash_type=K.KUQCD_HISQPC_DIRAC, inverter_type=K.KUQCD_CGM,
+                            matpc_type=K.KUQCD_EVEN_EVEN, prec=K.KUQCD_DOUBLE, num_shift=NSHIFT, max_iter=100000,
+                            iter=0, tol=(REL_RES ** 2) * bnorm2, shifts=C.cast(shc, C.POINTER(C.c_double)))
+    xs_np = [x.numpy() for x in hx_pin]
+    b_np = hb_pin.numpy()
+    with quiet_stdout():
+        for _ in range(max(1, args.warmup)):
+            assert K.kuqcd_solve_multishift(xs_np, b_np, ip) == 0
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            assert K.kuqcd_solve_multishift(xs_np, b_np, ip) == 0
+        e2e_s = (time.perf_counter() - t0) / args.steps
+    K.kuqcd_gauge_free()
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
     # the FP64 operator dominates every solver (the relaxed schedule runs it while |r| > rho32 |b|)
     dom = "fp64"
     peaks = {}
@@ -262,7 +281,8 @@ def run_ours(args):
 
     result = None
     if rank == 0:
-        cpu = cpu_baseline_sample(args) if (world == 1 and not args.no_cpu_baseline) else None
+        cpu = (cpu_baseline_sample(args, plain["iters"] if plain else None)
+               if (world == 1 and not args.no_cpu_baseline) else None)
         launches = main_run["launches"]
         plain_info = None
         if plain is not None:
@@ -287,8 +307,7 @@ def run_ours(args):
             "dtype": {"fp64": "f64", "fp64w": "f64", "mixed": "f64+f32", "mixed-half": "f64+f32+f16(int16+norm)"}[
                 args.solver],
             "data": "synthetic (seeded on device: exp(i eps H) thin links, Gaussian source)",
-            "config": {"workload": f"multishift CG {'x'.join(map(str, dims))}, {NSHIFT} shifts 1e-4..1, m={MASS}, "
-                                   f"eps={EPS}, per-shift true residual {REL_RES}",
+            "config": {"workload": workload_name(dims),
                        "solver": args.solver, "lattice": list(dims), "shifts": NSHIFT,
                        "iterations": iters[-1], "refine_iterations": main_run["refine"],
                        "max_true_residual": max(true_res), "sloppy_phase_residual": main_run["sloppy_res"],
@@ -309,32 +328,58 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
-    ctx.close()
     return result
 
 
 # ---------------------------------------------------------------------------------------------- CPU reference
 def ref_iterations_needed():
-    return REF_ITERS_32
+    return REF_ITERS
+
+
+class quiet_stdout:
+    """Send the C libraries' printf output (the reference's "CGM: # iterations" lines) to stderr, so that stdout
+    carries only the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+
+    def __exit__(self, *a):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+_REF_FIELDS = {}
 
 
 def ref_cpu_time_per_iter(dims, sample_iters, seed=1000):
-    """Time `sample_iters` iterations of the reference CGM (oracle/_ref, all host cores) on the bench workload."""
+    """Seconds per CGM iteration of the reference (oracle/_ref, all host cores) on the bench workload: the time of a
+    (1 + sample_iters)-iteration solve minus that of a 1-iteration solve, so that gauge loading, neighbour-table
+    construction and field copies (paid once per solve call) cancel."""
     from oracle import oracle as O
 
-    fat, lng = O.make_links(dims, EPS, seed)
-    b = O.make_source(dims, 0, seed)
+    key = (tuple(dims), seed)
+    if key not in _REF_FIELDS:
+        fat, lng = O.make_links(dims, EPS, seed)
+        _REF_FIELDS.clear()
+        _REF_FIELDS[key] = (fat, lng, O.make_source(dims, 0, seed))
+    fat, lng, b = _REF_FIELDS[key]
     sig = shifts_abs()
     refsh = [sig[0]] + [s - sig[0] for s in sig[1:]]
     tol = (REL_RES ** 2) * float(b @ b)
-    t0 = time.perf_counter()
-    st, xs, it = O.ref_solve(dims, fat, lng, b, refsh, tol, sample_iters)
-    t1 = time.perf_counter()
-    assert st == 0 and it == sample_iters
-    return (t1 - t0) / sample_iters
+    t = []
+    with quiet_stdout():
+        for n in (1, 1 + sample_iters):
+            t0 = time.perf_counter()
+            st, xs, it = O.ref_solve(dims, fat, lng, b, refsh, tol, n)
+            t.append(time.perf_counter() - t0)
+            assert st == 0 and it == n
+    return (t[1] - t[0]) / sample_iters
 
 
-def cpu_baseline_sample(args):
+def cpu_baseline_sample(args, iters_hint=None):
     from oracle import oracle as O
 
     if not O.ref_available():
@@ -342,7 +387,7 @@ def cpu_baseline_sample(args):
     dims = tuple(args.dims)
     sample = args.cpu_sample_iters
     t_it = ref_cpu_time_per_iter(dims, sample)
-    iters = ref_iterations_needed() or 0
+    iters = ref_iterations_needed() or iters_hint or 0
     solve_s = t_it * iters if iters else None
     return {"value": (1.0 / solve_s) if solve_s else None, "unit": "solves/s", "cores": os.cpu_count(),
             "kind": "reference", "seconds_per_iteration": t_it,
@@ -372,8 +417,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": solve_s * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": f"multishift CG {'x'.join(map(str, dims))}, {NSHIFT} shifts 1e-4..1, m={MASS}, "
-                               f"eps={EPS}, per-shift true residual {REL_RES}", "solver": "reference CGM (CPU)"},
+        "config": {"workload": workload_name(dims), "solver": "reference CGM (CPU)"},
         "cpu_baseline": {"value": v, "unit": "solves/s", "cores": os.cpu_count(), "kind": "reference",
                          "sample": f"{sample} CGM iterations per step, extrapolated to {iters} iterations"},
         "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -389,10 +433,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--solver", choices=["mixed", "mixed-half", "fp64", "fp64w"], default="mixed-half")
-    ap.add_argument("--dims", type=int, nargs=4, default=list(DIMS))
+    ap.add_argument("--config", choices=list(CONFIGS), default="32")
+    ap.add_argument("--dims", type=int, nargs=4, default=None, help="override the lattice of --config")
     ap.add_argument("--cpu-sample-iters", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    select_config(args.config)
+    if args.dims is None:
+        args.dims = list(DIMS)
     if args.impl == "reference":
         run_reference(args)
     else:
