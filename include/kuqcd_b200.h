@@ -126,6 +126,33 @@ KuQCDStatus kq_solve_multishift_device(kq_context *ctx, const kq_solve_param *pa
 KuQCDStatus kq_true_residuals(kq_context *ctx, int parity, int num_shift, const double *sigma, const void *d_b,
                               const void *d_x, double *out);
 
+/* ---------------------------------------------------------------- batched systems
+ * Many independent systems (each its own context: lattice, links; its own shifts and source) solved together: each
+ * kernel of an iteration is one persistent launch over all systems' site tiles, captured in CUDA graphs; launch
+ * shape autotuned and cached on disk (KUQCD_TUNE_CACHE).  No reference counterpart: the reference solves one
+ * system per kuqcd_solve_multishift call (kuqcd.cpp:404-445), so this replaces a loop of such calls. */
+typedef struct kq_batch kq_batch;
+typedef struct {
+    int num_systems;
+    int iterations;           /* largest iteration count over the systems */
+    double batched_seconds;   /* device time of the batched iterations */
+    long long kernel_launches;
+    int tile;                 /* sites per tile = threads per CTA */
+    int ctas_per_sm;          /* persistent grid: CTAs per SM */
+    double max_true_residual; /* over the KQ_SOLVER_MIXED systems' shifts (FP64, after any refinement) */
+    int refined_systems;      /* systems the FP64 check sent to refinement */
+    int tuned_now;            /* 1 when this call measured the launch shape */
+} kq_batch_info;
+
+KuQCDStatus kq_batch_create(int device, kq_batch **out);
+void kq_batch_destroy(kq_batch *b);
+/* d_b: FP64 device field of ctx; d_x: num_shift FP64 fields, kq_spinor_bytes(ctx, DOUBLE) apart.  solver:
+ * KQ_SOLVER_MIXED or KQ_SOLVER_CGM_WINDOWED.  ctx must hold FP64 links and outlive the batch. */
+KuQCDStatus kq_batch_add(kq_batch *b, kq_context *ctx, const kq_solve_param *param, const void *d_b, void *d_x);
+int kq_batch_size(const kq_batch *b);
+KuQCDStatus kq_batch_solve(kq_batch *b, kq_batch_info *info);
+KuQCDStatus kq_batch_system_info(const kq_batch *b, int i, kq_solve_info *out);
+
 /* ---------------------------------------------------------------- synthetic fields
  * thin U = exp(i eps H), H traceless Hermitian from seeded Gaussians; staggered phases folded in;
  * fat = 9/8 U, long = -1/24 U(x) U(x+mu) U(x+2mu); written as FP64 NORMAL_ORDER host records into DEVICE

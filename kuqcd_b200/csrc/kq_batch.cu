@@ -1,0 +1,692 @@
+// Batched multi-system multishift solver: many independent systems (own lattice, own links, own shifts, own source)
+// advanced together, every kernel of an iteration one persistent launch over a work list of (system, site tile)
+// items, W iterations captured in one CUDA graph.
+//
+// Why: one system of a small lattice (16^4: 32,768 sites per parity = 128 tiles) cannot fill 148 SMs, and a solve
+// of many small systems one after another is dominated by launch latency and tail effects.  Interleaving all
+// systems' tiles in each launch fills the GPU and amortises every launch over all systems.
+//
+// Each system runs the windowed multishift CG of kq_msrelax.cu (the CGM recurrences of inverter_cgm.cpp:17-87,
+// deferred shift updates, operator precision relaxed FP64 -> FP32 -> HALF as its own residual falls -- decided on
+// the device per system, kq_ms_device.cuh).  Reductions are per system: every tile publishes a partial sum and
+// the CTA that completes a system's last tile (per-system atomic ticket) runs that system's scalar step.
+// After the batched phase every system gets the FP64 true-residual check (and, if needed, the refinement) of the
+// single-system mixed solver.
+//
+// Tuning: tile size (threads per CTA) and resident CTAs per SM of the persistent grid are chosen by timing one
+// window of the actual batch (kq_tune.cu), cached on disk.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <mutex>
+#include <vector>
+
+#include "kq_context.h"
+#include "kq_dslash_core.cuh"
+#include "kq_ms_device.cuh"
+#include "kq_msrelax.h"
+#include "kq_tune.h"
+
+namespace kq {
+
+struct SysDesc {
+    Geom g;
+    int pv, parity, ntiles, pad;
+    LinkSet fat[3], lng[3];
+    const void *b;
+    void *x, *p0, *s, *tmp, *ring, *pw;
+    size_t vb;
+    double *partials;  // one per tile
+    MsState *st;
+};
+
+// The descriptors live in constant memory: every CTA works on one system at a time, so the (warp-uniform) indexed
+// constant loads are cheap and the fields need not be held in registers across the dslash (with the descriptors in
+// global memory the FP64 kernels needed ~40 more registers and lost occupancy).  One batch solves at a time per
+// process (kq_batch_solve holds a lock); at most kMaxBatch systems.
+constexpr int kMaxBatch = 128;
+__constant__ SysDesc c_sys[kMaxBatch];
+
+// ---------------------------------------------------------------------------------------------------- helpers
+__device__ __forceinline__ bool tile_ticket_last(unsigned *ticket, int ntiles)
+{
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == (unsigned)(ntiles - 1);
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
+__device__ __forceinline__ double tile_partials_sum(const double *p, int n, double *sm)
+{
+    double s = 0.0;
+    for (int b = threadIdx.x; b < n; b += blockDim.x) s += ((volatile const double *)p)[b];
+    return block_sum(s, sm);
+}
+
+// ---------------------------------------------------------------------------------------------------- kernels
+template <int BS>
+__global__ void __launch_bounds__(BS) bk_init_kernel(const SysDesc *__restrict__ sys, const int2 *__restrict__ items,
+                                                     int nitems)
+{
+    __shared__ double sm[32];
+#pragma unroll 1
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int2 w = items[it];
+        const SysDesc &d = c_sys[w.x];
+        MsState *st = d.st;
+        const int i = w.y * BS + threadIdx.x;
+        double nn = 0.0;
+        if (i < d.g.vh) {
+            double v[6], z[6] = {0, 0, 0, 0, 0, 0};
+            ld_spinor<0>(d.b, d.pv, i, v);
+            st_spinor<0>(d.p0, d.pv, i, v);
+            char *ring = static_cast<char *>(d.ring);
+            st_spinor<0>(ring, d.pv, i, v);
+            for (int l = 1; l < kWin; ++l) st_spinor<0>(ring + l * d.vb, d.pv, i, z);
+            for (int k = 0; k < st->ns; ++k) {
+                st_spinor<0>(static_cast<char *>(d.pw) + k * d.vb, d.pv, i, v);
+                st_spinor<0>(static_cast<char *>(d.x) + k * d.vb, d.pv, i, z);
+            }
+#pragma unroll
+            for (int e = 0; e < 6; ++e) nn += v[e] * v[e];
+        }
+        nn = block_sum(nn, sm);
+        if (threadIdx.x == 0) d.partials[w.y] = nn;
+        if (tile_ticket_last(&st->ticket[0], d.ntiles)) {
+            const double tot = tile_partials_sum(d.partials, d.ntiles, sm);
+            if (threadIdx.x == 0) {
+                st->rNorm2 = tot;
+                st->bnorm2 = tot;
+                // a negative tol is a relative stopping point: tol = (rel |b|)^2
+                if (st->tol < 0.0) st->tol = st->tol * st->tol * tot;
+                st->Bm1 = 1.0;
+                for (int k = 0; k < st->ns; ++k) {
+                    st->a[k] = 0.0;
+                    st->B[k] = 1.0;
+                    st->Z[k] = 1.0;
+                    st->Zm1[k] = 1.0;
+                }
+                st->maxTerm = st->ns;
+                st->wmax = st->ns;
+                st->iter = st->wpos = st->nupd = st->halt = st->status = 0;
+                st->mode = 0;
+                st->active = tot > 0.0 ? 1 : 0;
+                if (!st->active && st->running) atomicSub(st->running, 1);
+                st->ticket[0] = 0;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// K1: tmp = D p0 for the systems whose operator precision is M (one launch per precision, so that each launch is
+// specialised; systems in the other precisions skip their items)
+template <int BS, int M>
+__global__ void __launch_bounds__(BS, 768 / BS) bk_dslash1_kernel(const SysDesc *__restrict__ sys,
+                                                        const int2 *__restrict__ items, int nitems)
+{
+    typedef typename Acc2<M, M>::T T;
+#pragma unroll 1
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int2 w = items[it];
+        const SysDesc &d = c_sys[w.x];
+        const MsState *st = d.st;
+        if (!st->active || st->mode != M) continue;
+        const int i = w.y * BS + threadIdx.x;
+        if (i >= d.g.vh) continue;
+        T acc[6];
+        dslash_site_t<M, 0, T>(d.g, d.pv, d.fat[M], d.lng[M], d.p0, 1 - d.parity, i, acc);
+        st_spinor_as<M>(d.tmp, d.pv, i, acc);
+    }
+}
+
+// K2: s = sigma0 p0 - D tmp (FP64), <p0, s> -> beta step, for the systems in precision M
+template <int BS, int M>
+__global__ void __launch_bounds__(BS, 768 / BS) bk_dslash2_kernel(const SysDesc *__restrict__ sys,
+                                                        const int2 *__restrict__ items, int nitems)
+{
+    typedef typename Acc2<M, M>::T T;
+    __shared__ double sm[32];
+#pragma unroll 1
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int2 w = items[it];
+        const SysDesc &d = c_sys[w.x];
+        MsState *st = d.st;
+        if (!st->active || st->mode != M) continue;
+        const int i = w.y * BS + threadIdx.x;
+        double dot = 0.0;
+        if (i < d.g.vh) {
+            T acc[6];
+            dslash_site_t<M, M, T>(d.g, d.pv, d.fat[M], d.lng[M], d.tmp, d.parity, i, acc);
+            double pv6[6], sv[6];
+            ld_spinor<0>(d.p0, d.pv, i, pv6);
+            const double sig = st->shift[0];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                sv[k] = sig * pv6[k] - (double)acc[k];
+                dot += pv6[k] * sv[k];
+            }
+            st_spinor<0>(d.s, d.pv, i, sv);
+        }
+        dot = block_sum(dot, sm);
+        if (threadIdx.x == 0) d.partials[w.y] = dot;
+        if (tile_ticket_last(&st->ticket[1], d.ntiles)) {
+            const double tot = tile_partials_sum(d.partials, d.ntiles, sm);
+            if (threadIdx.x == 0) {
+                ms_step_beta(st, tot);
+                st->ticket[1] = 0;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// K3: r^(i) = r^(i-1) + B0 s into the ring, |r|^2 -> alpha step (and the next operator precision)
+template <int BS>
+__global__ void __launch_bounds__(BS) bk_r_kernel(const SysDesc *__restrict__ sys, const int2 *__restrict__ items,
+                                                  int nitems)
+{
+    __shared__ double sm[32];
+#pragma unroll 1
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int2 w = items[it];
+        const SysDesc &d = c_sys[w.x];
+        MsState *st = d.st;
+        if (!st->active) continue;
+        const int itc = st->iter;
+        const char *rin = static_cast<const char *>(d.ring) + (size_t)(itc % kWin) * d.vb;
+        char *rout = static_cast<char *>(d.ring) + (size_t)((itc + 1) % kWin) * d.vb;
+        const int i = w.y * BS + threadIdx.x;
+        double nn = 0.0;
+        if (i < d.g.vh) {
+            double rv[6], sv[6];
+            ld_spinor<0>(rin, d.pv, i, rv);
+            ld_spinor<0>(d.s, d.pv, i, sv);
+            const double b0 = st->B[0];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                rv[k] += b0 * sv[k];
+                nn += rv[k] * rv[k];
+            }
+            st_spinor<0>(rout, d.pv, i, rv);
+        }
+        nn = block_sum(nn, sm);
+        if (threadIdx.x == 0) d.partials[w.y] = nn;
+        if (tile_ticket_last(&st->ticket[2], d.ntiles)) {
+            const double tot = tile_partials_sum(d.partials, d.ntiles, sm);
+            if (threadIdx.x == 0) {
+                ms_step_alpha(st, tot);
+                st->ticket[2] = 0;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// K4: p0 = r^(i) + a0 p0.  A system that stopped in K3 no longer needs p0.
+template <int BS>
+__global__ void __launch_bounds__(BS) bk_p0_kernel(const SysDesc *__restrict__ sys, const int2 *__restrict__ items,
+                                                   int nitems)
+{
+#pragma unroll 1
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int2 w = items[it];
+        const SysDesc &d = c_sys[w.x];
+        const MsState *st = d.st;
+        if (!st->active) continue;
+        const int i = w.y * BS + threadIdx.x;
+        if (i >= d.g.vh) continue;
+        const char *r = static_cast<const char *>(d.ring) + (size_t)(st->iter % kWin) * d.vb;
+        double rv[6], pv6[6];
+        ld_spinor<0>(r, d.pv, i, rv);
+        ld_spinor<0>(d.p0, d.pv, i, pv6);
+        const double a0 = st->a[0];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) pv6[k] = rv[k] + a0 * pv6[k];
+        st_spinor<0>(d.p0, d.pv, i, pv6);
+    }
+}
+
+// K5: windowed shift update of every system that iterated in this window
+template <int BS>
+__global__ void __launch_bounds__(BS) bk_window_kernel(const SysDesc *__restrict__ sys,
+                                                       const int2 *__restrict__ items, int nitems)
+{
+    __shared__ double sc[kMaxShift], se[kMaxShift], sd[kMaxShift][kWin], sf[kMaxShift][kWin];
+#pragma unroll 1
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int2 w = items[it];
+        const SysDesc &d = c_sys[w.x];
+        MsState *st = d.st;
+        const int n = st->wpos, kmax = st->wmax;
+        if (n == 0) continue;  // uniform per system: nothing happened in this window
+        __syncthreads();
+        for (int t = threadIdx.x; t < kmax; t += BS) {
+            sc[t] = st->c[t];
+            se[t] = st->e[t];
+            for (int l = 0; l < kWin; ++l) {
+                sd[t][l] = st->d[t][l];
+                sf[t][l] = st->f[t][l];
+            }
+        }
+        __syncthreads();
+        const int i = w.y * BS + threadIdx.x;
+        if (i < d.g.vh)
+            window_update_site(static_cast<const char *>(d.ring), d.vb, d.pv, i, n, kmax, sc, se, sd, sf,
+                               static_cast<char *>(d.pw), static_cast<char *>(d.x));
+        if (tile_ticket_last(&st->ticket[0], d.ntiles)) {
+            if (threadIdx.x == 0) {
+                st->wpos = 0;
+                st->ticket[0] = 0;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------- host
+template <int BS>
+static void enqueue_batch_init(const SysDesc *d, const int2 *items, int nitems, int grid, cudaStream_t s)
+{
+    bk_init_kernel<BS><<<grid, BS, 0, s>>>(d, items, nitems);
+}
+
+template <int BS>
+static void enqueue_batch_chunk(const SysDesc *d, const int2 *items, int nitems, int grid, cudaStream_t s)
+{
+    for (int it = 0; it < kWin; ++it) {
+        bk_dslash1_kernel<BS, 0><<<grid, BS, 0, s>>>(d, items, nitems);
+        bk_dslash1_kernel<BS, 1><<<grid, BS, 0, s>>>(d, items, nitems);
+        bk_dslash1_kernel<BS, 2><<<grid, BS, 0, s>>>(d, items, nitems);
+        bk_dslash2_kernel<BS, 0><<<grid, BS, 0, s>>>(d, items, nitems);
+        bk_dslash2_kernel<BS, 1><<<grid, BS, 0, s>>>(d, items, nitems);
+        bk_dslash2_kernel<BS, 2><<<grid, BS, 0, s>>>(d, items, nitems);
+        bk_r_kernel<BS><<<grid, BS, 0, s>>>(d, items, nitems);
+        bk_p0_kernel<BS><<<grid, BS, 0, s>>>(d, items, nitems);
+    }
+    bk_window_kernel<BS><<<grid, BS, 0, s>>>(d, items, nitems);
+}
+
+}  // namespace kq
+
+using namespace kq;
+
+struct BatchSystem {
+    kq_context *ctx;
+    kq_solve_param param;
+    std::vector<double> shifts;
+    const void *d_b;
+    void *d_x;
+    kq_solve_info info;
+};
+
+struct kq_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<BatchSystem> sys;
+    void *work = nullptr;
+    size_t work_bytes = 0;
+    int *d_running = nullptr;
+    int *h_running = nullptr;  // pinned
+    SysDesc *d_desc = nullptr;
+    int2 *d_items = nullptr;
+    size_t items_cap = 0, desc_cap = 0;
+};
+
+#define KQ_API extern "C" __attribute__((visibility("default")))
+
+KQ_API KuQCDStatus kq_batch_create(int device, kq_batch **out)
+{
+    if (!out) return KUQCD_ERR_NULL_POINTER;
+    kq_batch *b = new (std::nothrow) kq_batch();
+    if (!b) return KUQCD_ERR_NO_MEMORY;
+    b->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_running, sizeof(int) * 4);
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_running, sizeof(int) * 4);
+    if (e != cudaSuccess) {
+        set_last_error(std::string("kq_batch_create: ") + cudaGetErrorString(e));
+        delete b;
+        return status_of(e);
+    }
+    *out = b;
+    return KUQCD_SUCCESS;
+}
+
+KQ_API void kq_batch_destroy(kq_batch *b)
+{
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->work) cudaFree(b->work);
+    if (b->d_desc) cudaFree(b->d_desc);
+    if (b->d_items) cudaFree(b->d_items);
+    if (b->d_running) cudaFree(b->d_running);
+    if (b->h_running) cudaFreeHost(b->h_running);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+KQ_API KuQCDStatus kq_batch_add(kq_batch *b, kq_context *ctx, const kq_solve_param *param, const void *d_b,
+                                void *d_x)
+{
+    if (!b || !ctx || !param || !param->shifts || !d_b || !d_x) {
+        set_last_error("kq_batch_add: null pointer");
+        return KUQCD_ERR_NULL_POINTER;
+    }
+    if (param->num_shift < 1 || param->num_shift > kMaxShift || (param->parity != 0 && param->parity != 1)) {
+        set_last_error("kq_batch_add: num_shift must be 1..64 and parity 0 or 1");
+        return KUQCD_ERR_INVALID_PARAM;
+    }
+    if (param->solver != KQ_SOLVER_MIXED && param->solver != KQ_SOLVER_CGM_WINDOWED) {
+        set_last_error("kq_batch_add: batched systems use KQ_SOLVER_MIXED or KQ_SOLVER_CGM_WINDOWED");
+        return KUQCD_ERR_UNSUPPORTED;
+    }
+    if (ctx->device != b->device) {
+        set_last_error("kq_batch_add: context on another device");
+        return KUQCD_ERR_INVALID_PARAM;
+    }
+    if (!ctx->fat_loaded || !ctx->long_loaded || ctx->master != P64) {
+        set_last_error("kq_batch_add: load FP64 fat and long links into the context first");
+        return KUQCD_ERR_UNEXPECTED_CALL_ORDER;
+    }
+    BatchSystem s;
+    s.ctx = ctx;
+    s.param = *param;
+    s.shifts.assign(param->shifts, param->shifts + param->num_shift);
+    s.param.shifts = nullptr;
+    s.d_b = d_b;
+    s.d_x = d_x;
+    memset(&s.info, 0, sizeof(s.info));
+    if ((int)b->sys.size() >= kMaxBatch) {
+        set_last_error("kq_batch_add: at most 128 systems per batch");
+        return KUQCD_ERR_UNSUPPORTED;
+    }
+    b->sys.push_back(s);
+    return KUQCD_SUCCESS;
+}
+
+KQ_API int kq_batch_size(const kq_batch *b) { return b ? (int)b->sys.size() : 0; }
+
+KQ_API KuQCDStatus kq_batch_system_info(const kq_batch *b, int i, kq_solve_info *out)
+{
+    if (!b || !out) return KUQCD_ERR_NULL_POINTER;
+    if (i < 0 || i >= (int)b->sys.size()) return KUQCD_ERR_INVALID_PARAM;
+    *out = b->sys[i].info;
+    return KUQCD_SUCCESS;
+}
+
+namespace {
+
+struct BatchPlan {
+    std::vector<SysDesc> desc;
+    std::vector<int2> items;
+    std::vector<MsState> init;
+};
+
+// Lay out every system's buffers in the batch workspace and build descriptors, work items and initial states.
+cudaError_t batch_plan(kq_batch *b, int bs, BatchPlan &plan, bool carve_only, size_t *bytes)
+{
+    Carve c(carve_only ? nullptr : b->work);
+    plan.desc.clear();
+    plan.items.clear();
+    plan.init.clear();
+    for (size_t si = 0; si < b->sys.size(); ++si) {
+        BatchSystem &S = b->sys[si];
+        kq_context *ctx = S.ctx;
+        const Geom &g = ctx->g;
+        const int ns = S.param.num_shift;
+        SysDesc d;
+        memset(&d, 0, sizeof(d));
+        d.g = g;
+        d.pv = pad_sites(g.vh);
+        d.parity = S.param.parity;
+        d.ntiles = (g.vh + bs - 1) / bs;
+        for (int p = 0; p < 3; ++p) {
+            d.fat[p] = ctx->gd.fat[p];
+            d.lng[p] = ctx->gd.lng[p];
+        }
+        const size_t vb = spinor_bytes(g, P64);
+        d.vb = vb;
+        d.b = S.d_b;
+        d.x = S.d_x;
+        d.p0 = c.take(vb);
+        d.s = c.take(vb);
+        d.tmp = c.take(vb);
+        d.ring = c.take(vb * kWin);
+        d.pw = c.take(vb * ns);
+        d.partials = static_cast<double *>(c.take(sizeof(double) * d.ntiles));
+        d.st = static_cast<MsState *>(c.take(sizeof(MsState)));
+        plan.desc.push_back(d);
+        for (int t = 0; t < d.ntiles; ++t) plan.items.push_back(make_int2((int)si, t));
+        MsState h;
+        memset(&h, 0, sizeof(h));
+        h.ns = ns;
+        h.max_iter = S.param.max_iter > 0 ? S.param.max_iter : 100000;
+        std::vector<double> sig(ns);
+        for (int k = 0; k < ns; ++k)
+            sig[k] = (S.param.shift_mode == 0 && k > 0) ? S.shifts[0] + S.shifts[k] : S.shifts[k];
+        h.shift[0] = sig[0];
+        for (int k = 1; k < ns; ++k) h.shift[k] = sig[k] - sig[0];
+        if (S.param.solver == KQ_SOLVER_MIXED) {
+            // the single-system mixed solver's schedule (kq_mixed.cu): stop at 0.7 x target, FP32 from
+            // 0.3 target / 1e-5, HALF from 0.3 target / 1e-3
+            const double tgt = S.param.rel_residual > 0 ? S.param.rel_residual : 1e-10;
+            h.tol = -0.7 * tgt;  // relative: the init kernel turns it into (0.7 tgt |b|)^2
+            const double r32 = 0.3 * tgt / 1e-5, r16 = 0.3 * tgt / 1e-3;
+            h.rho32_2 = r32 * r32;
+            h.rho16_2 = prec_from_api(S.param.prec) == P16 ? r16 * r16 : 0.0;
+        } else {
+            h.tol = S.param.tol;
+        }
+        h.running = b->d_running;
+        plan.init.push_back(h);
+    }
+    *bytes = c.off;
+    return cudaSuccess;
+}
+
+}  // namespace
+
+static std::mutex g_batch_mu;  // the descriptor table in constant memory is shared by all batches
+
+KQ_API KuQCDStatus kq_batch_solve(kq_batch *b, kq_batch_info *out)
+{
+    if (!b) return KUQCD_ERR_NULL_POINTER;
+    std::lock_guard<std::mutex> lk(g_batch_mu);
+    if (b->sys.empty()) {
+        set_last_error("kq_batch_solve: empty batch");
+        return KUQCD_ERR_INVALID_PARAM;
+    }
+    cudaSetDevice(b->device);
+    cudaStream_t s = b->stream;
+    // links the schedules need
+    for (auto &S : b->sys) {
+        const bool mixed = S.param.solver == KQ_SOLVER_MIXED;
+        const int precs[3] = {KUQCD_DOUBLE, KUQCD_SINGLE, KUQCD_HALF};
+        const int need = mixed ? (prec_from_api(S.param.prec) == P16 ? 3 : 2) : 1;
+        for (int p = 0; p < need; ++p) {
+            KuQCDStatus st = kq_prepare_links(S.ctx, precs[p]);
+            if (st != KUQCD_SUCCESS) return st;
+        }
+    }
+    int dev_sms = 148;
+    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, b->device);
+
+    // launch shape: tuned once per batch signature (sizes, shifts, schedule), cached on disk
+    std::string key = "batch";
+    for (auto &S : b->sys)
+        key += "_" + std::to_string(S.ctx->g.n[0]) + "x" + std::to_string(S.ctx->g.n[1]) + "x" +
+               std::to_string(S.ctx->g.n[2]) + "x" + std::to_string(S.ctx->g.n[3]) + "s" +
+               std::to_string(S.param.num_shift) + "m" + std::to_string(S.param.solver) + "p" +
+               std::to_string(S.param.prec);
+    BatchTune tune;
+    const bool have_tune = tune_lookup(key, &tune);
+    if (!have_tune) {
+        tune.bs = 256;
+        tune.ctas_per_sm = 4;
+    }
+
+    auto run = [&](int bs, int cps, int max_chunks, float *ms_out, long long *launches, int *chunks_out) -> cudaError_t {
+        BatchPlan plan;
+        size_t bytes = 0;
+        batch_plan(b, bs, plan, true, &bytes);
+        if (b->work_bytes < bytes) {
+            if (b->work) cudaFree(b->work);
+            b->work = nullptr;
+            b->work_bytes = 0;
+            KQ_CUDA_TRY(cudaMalloc(&b->work, bytes));
+            b->work_bytes = bytes;
+        }
+        batch_plan(b, bs, plan, false, &bytes);
+        const size_t nsys = plan.desc.size(), nit = plan.items.size();
+        if (b->desc_cap < nsys) {
+            if (b->d_desc) cudaFree(b->d_desc);
+            KQ_CUDA_TRY(cudaMalloc(&b->d_desc, sizeof(SysDesc) * nsys));
+            b->desc_cap = nsys;
+        }
+        if (b->items_cap < nit) {
+            if (b->d_items) cudaFree(b->d_items);
+            KQ_CUDA_TRY(cudaMalloc(&b->d_items, sizeof(int2) * nit));
+            b->items_cap = nit;
+        }
+        KQ_CUDA_TRY(cudaMemcpyAsync(b->d_desc, plan.desc.data(), sizeof(SysDesc) * nsys, cudaMemcpyHostToDevice, s));
+        KQ_CUDA_TRY(cudaMemcpyToSymbolAsync(c_sys, plan.desc.data(), sizeof(SysDesc) * nsys, 0,
+                                            cudaMemcpyHostToDevice, s));
+        KQ_CUDA_TRY(cudaMemcpyAsync(b->d_items, plan.items.data(), sizeof(int2) * nit, cudaMemcpyHostToDevice, s));
+        for (size_t i = 0; i < nsys; ++i)
+            KQ_CUDA_TRY(cudaMemcpyAsync(plan.desc[i].st, &plan.init[i], sizeof(MsState), cudaMemcpyHostToDevice, s));
+        const int nsys_i = (int)nsys;
+        KQ_CUDA_TRY(cudaMemcpyAsync(b->d_running, &nsys_i, sizeof(int), cudaMemcpyHostToDevice, s));
+        const int grid = std::max(1, std::min((int)nit, dev_sms * cps));
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        if (bs == 128) enqueue_batch_init<128>(b->d_desc, b->d_items, (int)nit, grid, s);
+        else enqueue_batch_init<256>(b->d_desc, b->d_items, (int)nit, grid, s);
+        KQ_CUDA_TRY(cudaGetLastError());
+        *launches = 1;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        KQ_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        if (bs == 128) enqueue_batch_chunk<128>(b->d_desc, b->d_items, (int)nit, grid, s);
+        else enqueue_batch_chunk<256>(b->d_desc, b->d_items, (int)nit, grid, s);
+        cudaError_t ee = cudaStreamEndCapture(s, &graph);
+        if (ee == cudaSuccess) ee = cudaGraphInstantiate(&exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        KQ_CUDA_TRY(ee);
+        int chunks = 0;
+        cudaError_t err = cudaSuccess;
+        cudaEventRecord(e0, s);  // device time of the iterations (after the init kernel and graph set-up)
+        for (;;) {
+            err = cudaMemcpyAsync(b->h_running, b->d_running, sizeof(int), cudaMemcpyDeviceToHost, s);
+            if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+            if (err != cudaSuccess || *b->h_running <= 0) break;
+            if (max_chunks > 0 && chunks >= max_chunks) break;
+            err = cudaGraphLaunch(exec, s);
+            if (err != cudaSuccess) break;
+            ++chunks;
+            *launches += 8 * kWin + 1;  // two dslash steps x three precisions + r + p0 per iteration, + window
+            if (chunks > 1000000) break;
+        }
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(ms_out, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaGraphExecDestroy(exec);
+        *chunks_out = chunks;
+        return err;
+    };
+
+    if (!have_tune) {
+        // time two windows of the real batch for every candidate shape; the solve restarts afterwards
+        float best = 1e30f;
+        const int bss[2] = {128, 256}, cpss[4] = {2, 4, 8, 16};
+        for (int bs : bss)
+            for (int cps : cpss) {
+                if (bs == 256 && cps > 8) continue;
+                float ms = 0;
+                long long l = 0;
+                int ch = 0;
+                cudaError_t e = run(bs, cps, 2, &ms, &l, &ch);
+                if (e != cudaSuccess) return status_of(e);
+                if (ch > 0 && ms < best) {
+                    best = ms;
+                    tune.bs = bs;
+                    tune.ctas_per_sm = cps;
+                }
+            }
+        tune_store(key, tune);
+    }
+    float ms = 0;
+    long long launches = 0;
+    int chunks = 0;
+    cudaError_t e = run(tune.bs, tune.ctas_per_sm, 0, &ms, &launches, &chunks);
+    if (e != cudaSuccess) {
+        set_last_error(std::string("kq_batch_solve: ") + cudaGetErrorString(e));
+        return status_of(e);
+    }
+    // per-system results, then the FP64 check / refinement of the mixed systems
+    BatchPlan plan;
+    size_t bytes = 0;
+    batch_plan(b, tune.bs, plan, false, &bytes);
+    int refined = 0;
+    double worst = 0.0;
+    int maxit = 0;
+    for (size_t i = 0; i < b->sys.size(); ++i) {
+        BatchSystem &S = b->sys[i];
+        MsState h;
+        const cudaError_t ec = cudaMemcpy(&h, plan.desc[i].st, sizeof(MsState), cudaMemcpyDeviceToHost);
+        if (ec != cudaSuccess) {
+            set_last_error(std::string("kq_batch_solve: ") + cudaGetErrorString(ec));
+            return status_of(ec);
+        }
+        memset(&S.info, 0, sizeof(S.info));
+        S.info.iter = h.iter;
+        S.info.status = h.status;
+        S.info.num_shift = S.param.num_shift;
+        maxit = std::max(maxit, h.iter);
+        if (S.param.solver == KQ_SOLVER_MIXED) {
+            std::vector<double> sig(S.param.num_shift);
+            for (int k = 0; k < S.param.num_shift; ++k)
+                sig[k] = (S.param.shift_mode == 0 && k > 0) ? S.shifts[0] + S.shifts[k] : S.shifts[k];
+            kq_solve_param p = S.param;
+            p.shifts = S.shifts.data();
+            kq_solve_info ri;
+            memset(&ri, 0, sizeof(ri));
+            cudaSetDevice(S.ctx->device);
+            cudaError_t e2 = mixed_solve(S.ctx, &p, sig.data(), S.d_b, S.d_x, &ri, false);
+            if (e2 != cudaSuccess) return status_of(e2);
+            S.info.iter_refine = ri.iter_refine;
+            S.info.kernel_launches = ri.kernel_launches;
+            for (int k = 0; k < S.param.num_shift; ++k) {
+                S.info.true_residual[k] = ri.true_residual[k];
+                worst = std::max(worst, ri.true_residual[k]);
+            }
+            if (ri.iter_refine > 0) ++refined;
+            if (ri.status) S.info.status = ri.status;
+        }
+    }
+    if (out) {
+        memset(out, 0, sizeof(*out));
+        out->num_systems = (int)b->sys.size();
+        out->iterations = maxit;
+        out->batched_seconds = ms * 1e-3;
+        out->kernel_launches = launches;
+        out->tile = tune.bs;
+        out->ctas_per_sm = tune.ctas_per_sm;
+        out->max_true_residual = worst;
+        out->refined_systems = refined;
+        out->tuned_now = have_tune ? 0 : 1;
+    }
+    return KUQCD_SUCCESS;
+}

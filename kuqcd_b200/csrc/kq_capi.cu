@@ -22,8 +22,6 @@ const char *last_error() { return g_last_error.c_str(); }
 
 cudaError_t launch_mdagm(const Geom &g, const GaugeDev &gd, int prec, double sigma, const void *src, void *tmp,
                          void *dst, int parity, cudaStream_t s);
-cudaError_t mixed_solve(struct ::kq_context *ctx, const kq_solve_param *param, const double *shifts_abs,
-                        const void *d_b, void *d_x, kq_solve_info *info);
 cudaError_t true_residuals(const Geom &g, const GaugeDev &gd, int parity, int ns, const double *sigma,
                            const void *d_b, const void *d_x, size_t xstride, void *d_tmp, void *d_s, double *partials,
                            double *out, cudaStream_t s);
@@ -394,7 +392,7 @@ KQ_API KuQCDStatus kq_solve_multishift_device(kq_context *ctx, const kq_solve_pa
     cudaEventRecord(e0, ctx->stream);
     cudaError_t e = cudaSuccess;
     if (p->solver == KQ_SOLVER_MIXED) {
-        e = mixed_solve(ctx, p, sig, d_b, d_x, info);
+        e = mixed_solve(ctx, p, sig, d_b, d_x, info, true);
     } else if (p->solver == KQ_SOLVER_CGM_WINDOWED) {
         MsBuffers w;
         Carve probe(nullptr);

@@ -37,4 +37,9 @@ struct Carve {
 cudaError_t ensure_work(::kq_context *ctx, size_t bytes);
 KuQCDStatus status_of(cudaError_t e);
 
+// KQ_SOLVER_MIXED on one context (kq_mixed.cu); shifts_abs are absolute.  With run_phase1 = false, d_x already
+// holds a multishift solution and only the FP64 check / refinement runs.
+cudaError_t mixed_solve(::kq_context *ctx, const kq_solve_param *param, const double *shifts_abs, const void *d_b,
+                        void *d_x, kq_solve_info *info, bool run_phase1);
+
 }  // namespace kq

@@ -412,8 +412,10 @@ static double env_double(const char *name, double dflt)
     return v ? atof(v) : dflt;
 }
 
+// run_phase1 = false: d_x already holds a multishift solution (the batched solver's); only the FP64 check and the
+// refinement of shifts above the target run.
 cudaError_t mixed_solve(::kq_context *ctx, const kq_solve_param *param, const double *sig, const void *d_b,
-                        void *d_x, kq_solve_info *info)
+                        void *d_x, kq_solve_info *info, bool run_phase1)
 {
     const Geom &g = ctx->g;
     cudaStream_t s = ctx->stream;
@@ -503,11 +505,13 @@ cudaError_t mixed_solve(::kq_context *ctx, const kq_solve_param *param, const do
         for (int k = 1; k < ns; ++k) rs[k] = sig[k] - sig[0];
         const double rho32 = relax_frac * target / eps32;
         const double rho16 = lp == P16 ? relax_frac * target / eps16 : 0.0;
-        MsResult r1;
-        KQ_CUDA_TRY(ms_solve(ctx, cw, param->parity, ns, rs, stop_frac * stop_frac * target * target * bb,
-                             param->max_iter > 0 ? param->max_iter : 100000, rho32, rho16, &r1));
-        info->iter = r1.iter;
-        launches += r1.launches;
+        if (run_phase1) {
+            MsResult r1;
+            KQ_CUDA_TRY(ms_solve(ctx, cw, param->parity, ns, rs, stop_frac * stop_frac * target * target * bb,
+                                 param->max_iter > 0 ? param->max_iter : 100000, rho32, rho16, &r1));
+            info->iter = r1.iter;
+            launches += r1.launches;
+        }
     }
 
     // ---- phase 2

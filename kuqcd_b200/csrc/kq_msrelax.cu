@@ -25,82 +25,12 @@
 
 #include "kq_context.h"
 #include "kq_dslash_core.cuh"
+#include "kq_ms_device.cuh"
 #include "kq_msrelax.h"
 
 namespace kq {
 
 constexpr int kBSm = 256;
-
-// ---------------------------------------------------------------------------------------------------- scalar steps
-__device__ void ms_step_beta(MsState *st, double pAp)
-{
-    st->pAp = pAp;
-    const double B0 = -st->rNorm2 / pAp;
-    if (!(pAp != 0.0) || !isfinite(B0)) {
-        st->status = KQ_STATUS_BREAKDOWN;
-        st->active = 0;
-        st->halt = 1;
-        return;
-    }
-    const int mt = st->maxTerm;
-    if (st->wpos == 0) {  // first iteration of a window: identity representation p = p_old, x = x_old
-        for (int k = 0; k < st->ns; ++k) {
-            st->c[k] = 1.0;
-            st->e[k] = 0.0;
-            for (int l = 0; l < kWin; ++l) st->d[k][l] = st->f[k][l] = 0.0;
-        }
-        st->wmax = mt;
-    }
-    st->B[0] = B0;
-    const double Bm1 = st->Bm1, a0 = st->a[0];
-    for (int j = 1; j < mt; ++j) {
-        const double rr1 = Bm1 * st->Zm1[j] /
-                           (B0 * a0 * (st->Zm1[j] - st->Z[j]) + st->Zm1[j] * Bm1 * (1.0 - st->shift[j] * B0));
-        st->Zm1[j] = st->Z[j];
-        st->Z[j] = st->Z[j] * rr1;
-        st->B[j] = B0 * rr1;
-    }
-    st->Bm1 = B0;
-    // x_k -= B_k p_k with p_k in its current window representation
-    const int jw = st->wpos;  // ring positions 0..jw-1 are in use
-    for (int k = 0; k < mt; ++k) {
-        const double Bk = st->B[k];
-        st->e[k] -= Bk * st->c[k];
-        for (int l = 0; l < jw; ++l) st->f[k][l] -= Bk * st->d[k][l];
-    }
-    st->nupd = mt;
-}
-
-__device__ void ms_step_alpha(MsState *st, double lambda2)
-{
-    st->lambda2 = lambda2;
-    st->a[0] = lambda2 / st->rNorm2;
-    st->rNorm2 = lambda2;
-    const int nu = st->nupd;
-    for (int j = 1; j < nu; ++j) st->a[j] = st->a[0] * st->Z[j] * st->B[j] / (st->Zm1[j] * st->B[0]);
-    // p_k = Z_k r^(new) + a_k p_k
-    const int jw = st->wpos;
-    for (int k = 0; k < nu; ++k) {
-        const double ak = st->a[k];
-        st->c[k] *= ak;
-        for (int l = 0; l < jw; ++l) st->d[k][l] *= ak;
-        st->d[k][jw] = st->Z[k];
-    }
-    int mt = st->maxTerm;
-    double lambda;
-    do {
-        lambda = st->Z[mt - 1] * st->Z[mt - 1] * lambda2;
-        if (lambda < st->tol) mt--;
-    } while (mt > 0 && lambda < st->tol);
-    st->maxTerm = mt;
-    st->iter += 1;
-    st->wpos = jw + 1;
-    if (!isfinite(lambda2)) {
-        st->status = KQ_STATUS_BREAKDOWN;
-        st->halt = 1;
-    }
-    st->active = (mt > 0 && st->iter < st->max_iter && !st->halt) ? 1 : 0;
-}
 
 // ---------------------------------------------------------------------------------------------------- kernels
 __global__ void __launch_bounds__(kBSm) ms_init_kernel(int vh, int pv, const void *__restrict__ b, char *x0,
@@ -255,35 +185,7 @@ __global__ void __launch_bounds__(kBSm) ms_window_kernel(int vh, int pv, const c
         }
         __syncthreads();
         const int i = blockIdx.x * kBSm + threadIdx.x;
-        if (i < vh) {
-            // window position l (0-based) holds r^(i0+l+1) in ring slot (l+1) % W
-            double rl[kWin][6];
-#pragma unroll
-            for (int l = 0; l < kWin; ++l) {
-                if (l < n) ld_spinor<0>(ring + (size_t)((l + 1) % kWin) * vb, pv, i, rl[l]);
-                else
-#pragma unroll
-                    for (int e = 0; e < 6; ++e) rl[l][e] = 0.0;
-            }
-            for (int k = 0; k < kmax; ++k) {
-                double pk[6], xk[6];
-                ld_spinor<0>(pw0 + k * vb, pv, i, pk);
-                ld_spinor<0>(x0 + k * vb, pv, i, xk);
-#pragma unroll
-                for (int e = 0; e < 6; ++e) {
-                    double pn = sc[k] * pk[e], xn = xk[e] + se[k] * pk[e];
-#pragma unroll
-                    for (int l = 0; l < kWin; ++l) {
-                        pn += sd[k][l] * rl[l][e];
-                        xn += sf[k][l] * rl[l][e];
-                    }
-                    pk[e] = pn;
-                    xk[e] = xn;
-                }
-                st_spinor<0>(pw0 + k * vb, pv, i, pk);
-                st_spinor<0>(x0 + k * vb, pv, i, xk);
-            }
-        }
+        if (i < vh) window_update_site(ring, vb, pv, i, n, kmax, sc, se, sd, sf, pw0, x0);
     }
     // last block resets the window
     __shared__ bool last;

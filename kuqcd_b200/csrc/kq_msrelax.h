@@ -18,6 +18,9 @@ struct MsState {
     double a[kMaxShift], B[kMaxShift], Z[kMaxShift], Zm1[kMaxShift];
     double c[kMaxShift], e[kMaxShift];           // p_k, x_k coefficients of p_k at the window start
     double d[kMaxShift][kWin], f[kMaxShift][kWin];  // coefficients of the ring residuals
+    int mode, pad3;           // operator precision of the next iteration (0 FP64, 1 FP32, 2 HALF; set on the device)
+    double rho32_2, rho16_2;  // squared relative-residual switch points (0: never)
+    int *running;             // batched solver: systems still iterating (decremented when this one stops)
 };
 
 struct MsPoll {

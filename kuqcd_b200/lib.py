@@ -64,8 +64,15 @@ EXPORTED_SYMBOLS = [
     "kq_spinor_bytes", "kq_spinor_upload", "kq_spinor_download", "kq_spinor_convert", "kq_dslash", "kq_mdagm",
     "kq_mdagm_noalloc",
     "kq_solve_multishift", "kq_solve_multishift_device", "kq_true_residuals", "kq_make_links_record",
-    "kq_make_source_record", "kq_last_error",
+    "kq_make_source_record", "kq_last_error", "kq_batch_create", "kq_batch_destroy", "kq_batch_add",
+    "kq_batch_size", "kq_batch_solve", "kq_batch_system_info",
 ]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("num_systems", C.c_int), ("iterations", C.c_int), ("batched_seconds", C.c_double),
+                ("kernel_launches", C.c_longlong), ("tile", C.c_int), ("ctas_per_sm", C.c_int),
+                ("max_true_residual", C.c_double), ("refined_systems", C.c_int), ("tuned_now", C.c_int)]
 
 _PKG = Path(__file__).resolve().parent
 lib_path = Path(os.environ.get("KUQCD_B200_LIB", _PKG / "libkuqcd_b200.so"))
@@ -111,6 +118,12 @@ def library() -> C.CDLL:
         "kq_make_links_record": (i, [vp, d, C.c_uint64, vp, vp]),
         "kq_make_source_record": (i, [vp, i, C.c_uint64, vp]),
         "kq_last_error": (C.c_char_p, []),
+        "kq_batch_create": (i, [i, C.POINTER(vp)]),
+        "kq_batch_destroy": (None, [vp]),
+        "kq_batch_add": (i, [vp, vp, C.POINTER(SolveParam), vp, vp]),
+        "kq_batch_size": (i, [vp]),
+        "kq_batch_solve": (i, [vp, C.POINTER(BatchInfo)]),
+        "kq_batch_system_info": (i, [vp, i, C.POINTER(SolveInfo)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -270,3 +283,48 @@ class Context:
 
     def make_source(self, parity: int, seed: int, d_b):
         self._chk(library().kq_make_source_record(self._h, parity, seed, _ptr(d_b)), "kq_make_source_record")
+
+
+class Batch:
+    """kq_batch: independent systems (each a Context with its own lattice and links) solved together."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        st = library().kq_batch_create(device, C.byref(h))
+        if st != 0:
+            raise KuQCDError(st, "kq_batch_create")
+        self._h = h
+        self._keep = []
+
+    def add(self, ctx: Context, d_b, d_x, shifts, parity=0, solver=KQ_SOLVER_MIXED, prec=KUQCD_HALF,
+            rel_residual=1e-10, tol=0.0, max_iter=100000, shift_mode=1):
+        p, sh = Context._param(shifts, parity, solver, prec, KUQCD_DOUBLE, max_iter, tol, rel_residual, shift_mode)
+        self._keep.append((ctx, d_b, d_x, sh))
+        st = library().kq_batch_add(self._h, ctx._h, C.byref(p), _ptr(d_b), _ptr(d_x))
+        if st != 0:
+            raise KuQCDError(st, "kq_batch_add")
+
+    def solve(self) -> BatchInfo:
+        info = BatchInfo()
+        st = library().kq_batch_solve(self._h, C.byref(info))
+        if st != 0:
+            raise KuQCDError(st, "kq_batch_solve")
+        return info
+
+    def system_info(self, i: int) -> SolveInfo:
+        info = SolveInfo()
+        st = library().kq_batch_system_info(self._h, i, C.byref(info))
+        if st != 0:
+            raise KuQCDError(st, "kq_batch_system_info")
+        return info
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library().kq_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,96 @@
+"""GPU tests of the batched multi-system solver (kq_batch_*): systems of different lattices, gauge fields, masses
+and shift sets solved in one set of persistent launches; every system checked against the oracle and against the
+single-system solver."""
+import numpy as np
+import pytest
+import torch
+
+import kuqcd_b200 as K
+from oracle import oracle as O
+
+SYSTEMS = [  # dims, eps, mass, shifts, parity, seed
+    ((4, 4, 4, 4), 0.2, 0.1, 8, 0, 11),
+    ((6, 6, 6, 6), 0.35, 0.03, 12, 1, 12),
+    ((8, 4, 4, 8), 0.4, 0.05, 16, 0, 13),
+    ((4, 4, 4, 1), 0.3, 0.07, 3, 1, 14),
+]
+
+
+def build(dims, eps, seed, parity):
+    fat, lng = O.make_links(dims, eps, seed)
+    ctx = K.Context(dims)
+    ctx.load_links(K.KUQCD_FAT_LINK, fat)
+    ctx.load_links(K.KUQCD_LONG_LINK, lng)
+    b = O.make_source(dims, parity, seed)
+    vb = ctx.spinor_bytes(K.KUQCD_DOUBLE)
+    d_b = torch.zeros(vb, dtype=torch.uint8, device="cuda")
+    ctx.upload(K.KUQCD_DOUBLE, b, d_b)
+    return ctx, fat, lng, b, d_b, vb
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("solver,prec", [(K.KQ_SOLVER_MIXED, K.KUQCD_HALF), (K.KQ_SOLVER_MIXED, K.KUQCD_SINGLE),
+                                         (K.KQ_SOLVER_CGM_WINDOWED, K.KUQCD_DOUBLE)])
+def test_batch_solves_every_system(cuda, tmp_path, monkeypatch, solver, prec):
+    monkeypatch.setenv("KUQCD_TUNE_CACHE", str(tmp_path / "tune.txt"))
+    batch = K.Batch()
+    keep = []
+    for dims, eps, mass, ns, parity, seed in SYSTEMS:
+        ctx, fat, lng, b, d_b, vb = build(dims, eps, seed, parity)
+        sig = list(mass * mass + np.logspace(-4, 0, ns))
+        d_x = torch.zeros(vb * ns, dtype=torch.uint8, device="cuda")
+        tol = (1e-10) ** 2 * float(b @ b)
+        batch.add(ctx, d_b, d_x, sig, parity=parity, solver=solver, prec=prec, rel_residual=1e-10, tol=tol)
+        keep.append((ctx, fat, lng, b, d_x, vb, sig, parity, dims))
+    info = batch.solve()
+    # the first solve of a signature measures the launch shape (unless this process already tuned it)
+    assert info.num_systems == len(SYSTEMS) and info.tile in (128, 256) and info.ctas_per_sm >= 1
+    for i, (ctx, fat, lng, b, d_x, vb, sig, parity, dims) in enumerate(keep):
+        si = batch.system_info(i)
+        assert si.status == 0, i
+        for k, s in enumerate(sig):
+            xk = ctx.download(K.KUQCD_DOUBLE, d_x[k * vb:(k + 1) * vb])
+            r = O.true_residual(dims, fat, lng, parity, s, b, xk)
+            assert r <= (1.2e-10 if solver == K.KQ_SOLVER_MIXED else 1.5e-10), (i, k, r)
+    # same batch again: the launch shape now comes from the cache
+    info2 = batch.solve()
+    assert info2.tuned_now == 0 and info2.tile == info.tile and info2.ctas_per_sm == info.ctas_per_sm
+    batch.close()
+
+
+@pytest.mark.gpu
+def test_batch_matches_single_system_solver(cuda, tmp_path, monkeypatch):
+    """KQ_SOLVER_CGM_WINDOWED in a batch runs the same recurrences as the single-system solver: same iteration
+    count, same solutions up to reduction order."""
+    monkeypatch.setenv("KUQCD_TUNE_CACHE", str(tmp_path / "tune.txt"))
+    dims, eps, mass, ns, parity, seed = SYSTEMS[1]
+    ctx, fat, lng, b, d_b, vb = build(dims, eps, seed, parity)
+    sig = list(mass * mass + np.logspace(-4, 0, ns))
+    tol = (1e-10) ** 2 * float(b @ b)
+    xs, single = ctx.solve(b, sig, parity=parity, solver=K.KQ_SOLVER_CGM_WINDOWED, tol=tol)
+    # a second, smaller system shares the launches
+    ctx2, _, _, b2, d_b2, vb2 = build((4, 4, 4, 4), 0.3, 99, 0)
+    batch = K.Batch()
+    d_x = torch.zeros(vb * ns, dtype=torch.uint8, device="cuda")
+    d_x2 = torch.zeros(vb2 * 4, dtype=torch.uint8, device="cuda")
+    batch.add(ctx, d_b, d_x, sig, parity=parity, solver=K.KQ_SOLVER_CGM_WINDOWED, tol=tol)
+    batch.add(ctx2, d_b2, d_x2, [0.01, 0.1, 0.5, 1.0], solver=K.KQ_SOLVER_CGM_WINDOWED,
+              tol=(1e-10) ** 2 * float(b2 @ b2))
+    batch.solve()
+    assert abs(batch.system_info(0).iter - single.iter) <= 1
+    for k in range(ns):
+        xb = ctx.download(K.KUQCD_DOUBLE, d_x[k * vb:(k + 1) * vb])
+        assert np.abs(xb - xs[k]).max() <= 1e-9 * np.abs(xs[k]).max(), k
+    batch.close()
+
+
+@pytest.mark.gpu
+def test_batch_argument_checks(cuda):
+    batch = K.Batch()
+    with pytest.raises(K.KuQCDError):
+        batch.solve()  # empty
+    ctx = K.Context((4, 4, 4, 4))  # no links
+    d = torch.zeros(16, dtype=torch.uint8, device="cuda")
+    with pytest.raises(K.KuQCDError):
+        batch.add(ctx, d, d, [0.1])
+    batch.close()
