@@ -153,6 +153,34 @@ int kq_batch_size(const kq_batch *b);
 KuQCDStatus kq_batch_solve(kq_batch *b, kq_batch_info *info);
 KuQCDStatus kq_batch_system_info(const kq_batch *b, int i, kq_solve_info *out);
 
+/* ---------------------------------------------------------------- learned preconditioner
+ * A gauge-covariant parallel-transport convolution network (layers of y_o = sum_i,p W[o][i][p] T_p v_i with the
+ * context's fat links as parallel transporters; BF16 tensor-core channel mixing, FP32 accumulation) trained on
+ * solver-generated residual/error pairs, used by a per-shift flexible-CG polish.  No reference counterpart (the
+ * reference's CGM is unpreconditioned, inverter_cgm.cpp:17-87). */
+typedef struct kq_net kq_net;
+/* channels[0..nlayers]: 1, 8, ..., 8, 1 */
+KuQCDStatus kq_net_create(kq_context *ctx, int nlayers, const int *channels, kq_net **out);
+void kq_net_destroy(kq_net *net);
+size_t kq_net_num_weights(const kq_net *net); /* floats: complex weights as (re, im) pairs, layers concatenated */
+KuQCDStatus kq_net_set_weights(kq_net *net, const float *w, size_t count);
+KuQCDStatus kq_net_get_weights(const kq_net *net, float *w, size_t count);
+KuQCDStatus kq_net_get_grad(const kq_net *net, float *grad, size_t count);
+KuQCDStatus kq_net_zero_grad(kq_net *net);
+/* switch to the links of another context of the same lattice */
+KuQCDStatus kq_net_set_context(kq_net *net, kq_context *ctx);
+/* d_out = N(d_in), FP64 fields of parity `parity` */
+KuQCDStatus kq_net_apply(kq_net *net, const void *d_in, void *d_out, int parity);
+/* one training pair: forward, loss |N(r) - e|^2 / e_norm2, backward; the weight gradient is accumulated */
+KuQCDStatus kq_net_train_pair(kq_net *net, const void *d_r, const void *d_e, int parity, double e_norm2,
+                              double *loss);
+/* Adam step on the accumulated gradient times grad_scale; clears the accumulator */
+KuQCDStatus kq_net_adam(kq_net *net, float lr, float grad_scale);
+/* Polish every shift of d_x (initial guesses, num_shift FP64 fields) to the FP64 true relative residual
+ * param->rel_residual with FCG preconditioned by net (NULL: plain CG, also the fallback on breakdown). */
+KuQCDStatus kq_fcg_polish(kq_context *ctx, kq_net *net, const kq_solve_param *param, const void *d_b, void *d_x,
+                          kq_solve_info *info);
+
 /* ---------------------------------------------------------------- synthetic fields
  * thin U = exp(i eps H), H traceless Hermitian from seeded Gaussians; staggered phases folded in;
  * fat = 9/8 U, long = -1/24 U(x) U(x+mu) U(x+2mu); written as FP64 NORMAL_ORDER host records into DEVICE

@@ -18,5 +18,5 @@ from .lib import (  # noqa: F401
     KUQCD_XYZT_ORDER, KUQCD_TZYX_ORDER, KQ_SOLVER_CGM, KQ_SOLVER_MIXED, KQ_SOLVER_CGM_WINDOWED,
     KuQCDGaugeParam, KuQCDInvertParam, SolveParam, SolveInfo, EXPORTED_SYMBOLS,
     library, lib_path, kuqcd_init, kuqcd_load_gaugefield, kuqcd_solve_multishift, kuqcd_gauge_free, kuqcd_end,
-    Context, KuQCDError, Batch, BatchInfo,
+    Context, KuQCDError, Batch, BatchInfo, Net, fcg_polish,
 )

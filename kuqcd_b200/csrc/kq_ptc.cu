@@ -1,0 +1,420 @@
+// Gauge-covariant parallel-transport convolution (PTC) network: the learned preconditioner of the FCG polish.
+// (No reference counterpart: the reference has no preconditioner, inverter_cgm.cpp:17-87.)
+//
+// Field of C channels on the full lattice (both parities), activation layout: plane ((c*2 + parity)*3 + colour) of
+// float2 (re, im) per checkerboard site, planes pv sites apart.  One layer, C_in -> C_out channels:
+//
+//   y_o(x) = sum_i sum_p W[o][i][p] (T_p v_i)(x)
+//   T_0 = 1,  T_{1+2mu} v (x) = F_mu(x) v(x+mu),  T_{2+2mu} v (x) = F_mu(x-mu)^dag v(x-mu)
+//
+// with the FP32 device fat links F (they carry the dslash's factor 1/2) and complex weights W.  Per tile of 128
+// sites of one parity the transported inputs are gathered in FP32, rounded to BF16 into shared memory, and the
+// channel mixing is a real GEMM per colour: [128 x K] x [K x N], K = C_in*9*2 (re, im), N = C_out*2, on the tensor
+// cores (mma.sync m16n8k16 BF16, FP32 accumulate).  The adjoint layer (for input gradients) is the same kernel with
+// weights W'[i][o][p'] = conj(W[o][i][p]) and forward/backward hops swapped.  The weight gradient dL/dB = T^T G is a
+// second tensor-core GEMM over the rows of each tile; per-tile partials are summed in a fixed order.
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kq_context.h"
+#include "kq_dslash_core.cuh"
+#include "kq_ptc.h"
+
+namespace kq {
+
+constexpr int kTile = 128;  // sites per CTA
+constexpr int kThr = 128;   // threads per CTA (4 warps)
+constexpr int kPaths = 9;
+
+__host__ __device__ constexpr int kpad_of(int cin) { return ((cin * kPaths * 2 + 15) / 16) * 16; }
+__host__ __device__ constexpr int npad_of(int cout) { return ((cout * 2 + 7) / 8) * 8; }
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
+{
+    __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t *>(&h);
+}
+
+__device__ __forceinline__ void mma_bf16(float d[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ float2 ld_act(const float2 *act, int pv, int c, int par, int a, int i)
+{
+    return __ldg(act + (size_t)((c * 2 + par) * 3 + a) * pv + i);
+}
+
+// Gather the transported inputs of site i (parity par) for all channels and paths and hand them, colour by colour,
+// to `put(colour, k, value)` with k = (c*9 + p)*2 + reim.
+template <int CIN, typename Put>
+__device__ __forceinline__ void gather_site(const Geom &g, int pv, const LinkSet &fat, const float2 *act, int par,
+                                            int i, bool swap_paths, Put put)
+{
+    const SiteCoord cd = site_coord(g, i, par);
+    const int q = 1 - par;
+    const void *fat_p = par ? fat.par[1] : fat.par[0];
+    const void *fat_q = par ? fat.par[0] : fat.par[1];
+    // identity path
+#pragma unroll
+    for (int c = 0; c < CIN; ++c)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float2 v = ld_act(act, pv, c, par, a, i);
+            put(a, (c * kPaths + 0) * 2 + 0, v.x);
+            put(a, (c * kPaths + 0) * 2 + 1, v.y);
+        }
+#pragma unroll 1
+    for (int dir = 0; dir < 4; ++dir) {
+#pragma unroll
+        for (int fb = 0; fb < 2; ++fb) {
+            // fb = 0: forward hop F(x) v(x+mu); fb = 1: backward hop F(x-mu)^dag v(x-mu)
+            const int nb = nbr_index(g, cd, i, dir, fb == 0 ? 1 : -1);
+            float u[18];
+            ld_link<1>(fb == 0 ? fat_p : fat_q, pv, dir, fb == 0 ? i : nb, 1.f, u);
+            // adjoint layers run the hops with swapped path labels
+            const int p = 1 + 2 * dir + (swap_paths ? 1 - fb : fb);
+#pragma unroll
+            for (int c = 0; c < CIN; ++c) {
+                float v[6], o[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    const float2 w = ld_act(act, pv, c, q, a, nb);
+                    v[2 * a] = w.x;
+                    v[2 * a + 1] = w.y;
+                }
+                if (fb == 0) mv_add(u, v, o);
+                else {
+                    mdv_sub(u, v, o);
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) o[k] = -o[k];
+                }
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    put(a, (c * kPaths + p) * 2 + 0, o[2 * a]);
+                    put(a, (c * kPaths + p) * 2 + 1, o[2 * a + 1]);
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------- forward
+// out (C_out channels, both parities) = layer(in); Bt: [N_pad][K_pad] BF16 weights (device), built by the host.
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kThr) ptc_forward_kernel(Geom g, int pv, LinkSet fat, const float2 *__restrict__ in,
+                                                           float2 *__restrict__ out, const __nv_bfloat16 *__restrict__ Bt,
+                                                           int swap_paths)
+{
+    constexpr int KP = kpad_of(CIN), NP = npad_of(COUT), KS = KP + 8;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __nv_bfloat16 *As = reinterpret_cast<__nv_bfloat16 *>(smem_raw);  // [3][kTile][KS]
+    __nv_bfloat16 *Bs = As + 3 * kTile * KS;                          // [NP][KS]
+    const int tiles_per_par = (g.vh + kTile - 1) / kTile;
+    const int par = blockIdx.x / tiles_per_par;
+    const int base = (blockIdx.x - par * tiles_per_par) * kTile;
+    const int t = threadIdx.x;
+    for (int e = t; e < NP * KP; e += kThr) {
+        const int n = e / KP, k = e - n * KP;
+        Bs[n * KS + k] = Bt[e];
+    }
+    const int i = base + t;
+    if (i < g.vh) {
+        gather_site<CIN>(g, pv, fat, in, par, i, swap_paths != 0, [&](int a, int k, float v) {
+            As[(a * kTile + t) * KS + k] = __float2bfloat16_rn(v);
+        });
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+            for (int k = CIN * kPaths * 2; k < KP; ++k) As[(a * kTile + t) * KS + k] = __float2bfloat16_rn(0.f);
+    } else {
+        for (int a = 0; a < 3; ++a)
+            for (int k = 0; k < KP; ++k) As[(a * kTile + t) * KS + k] = __float2bfloat16_rn(0.f);
+    }
+    __syncthreads();
+    const int warp = t >> 5, lane = t & 31, gq = lane >> 2, tq = lane & 3;
+#pragma unroll 1
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            const int r0 = warp * 32 + mt * 16;
+#pragma unroll
+            for (int nt = 0; nt < NP / 8; ++nt) {
+                float d[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                for (int ks = 0; ks < KP / 16; ++ks) {
+                    const __nv_bfloat16 *A0 = As + (a * kTile + r0 + gq) * KS + ks * 16 + 2 * tq;
+                    const __nv_bfloat16 *A1 = A0 + 8 * KS;
+                    const uint32_t a0 = *reinterpret_cast<const uint32_t *>(A0);
+                    const uint32_t a1 = *reinterpret_cast<const uint32_t *>(A1);
+                    const uint32_t a2 = *reinterpret_cast<const uint32_t *>(A0 + 8);
+                    const uint32_t a3 = *reinterpret_cast<const uint32_t *>(A1 + 8);
+                    const __nv_bfloat16 *B0 = Bs + (nt * 8 + gq) * KS + ks * 16 + 2 * tq;
+                    const uint32_t b0 = *reinterpret_cast<const uint32_t *>(B0);
+                    const uint32_t b1 = *reinterpret_cast<const uint32_t *>(B0 + 8);
+                    mma_bf16(d, a0, a1, a2, a3, b0, b1);
+                }
+                const int o = nt * 4 + tq;  // columns 2*tq, 2*tq+1 = (re, im) of channel o
+                if (o < COUT) {
+                    const int s0 = base + r0 + gq, s1 = s0 + 8;
+                    float2 *plane = out + (size_t)((o * 2 + par) * 3 + a) * pv;
+                    if (s0 < g.vh) plane[s0] = make_float2(d[0], d[1]);
+                    if (s1 < g.vh) plane[s1] = make_float2(d[2], d[3]);
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------- weight grad
+// partial[tile][k][n] = sum over the tile's rows (sites x colours) of T[row][k] * G[row][n]
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kThr) ptc_wgrad_kernel(Geom g, int pv, LinkSet fat, const float2 *__restrict__ in,
+                                                         const float2 *__restrict__ gout, float *__restrict__ partial)
+{
+    constexpr int KP = kpad_of(CIN), NP = npad_of(COUT), RS = kTile + 8;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __nv_bfloat16 *Tt = reinterpret_cast<__nv_bfloat16 *>(smem_raw);  // [3][KP][RS]
+    __nv_bfloat16 *Gt = Tt + 3 * KP * RS;                             // [3][NP][RS]
+    const int tiles_per_par = (g.vh + kTile - 1) / kTile;
+    const int par = blockIdx.x / tiles_per_par;
+    const int base = (blockIdx.x - par * tiles_per_par) * kTile;
+    const int t = threadIdx.x;
+    const int i = base + t;
+    for (int a = 0; a < 3; ++a)
+        for (int k = 0; k < KP; ++k) Tt[(a * KP + k) * RS + t] = __float2bfloat16_rn(0.f);
+    if (i < g.vh) {
+        gather_site<CIN>(g, pv, fat, in, par, i, false, [&](int a, int k, float v) {
+            Tt[(a * KP + k) * RS + t] = __float2bfloat16_rn(v);
+        });
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int n = 0; n < NP; ++n) {
+            float v = 0.f;
+            const int o = n >> 1;
+            if (i < g.vh && o < COUT) {
+                const float2 w = ld_act(gout, pv, o, par, a, i);
+                v = (n & 1) ? w.y : w.x;
+            }
+            Gt[(a * NP + n) * RS + t] = __float2bfloat16_rn(v);
+        }
+    __syncthreads();
+    const int warp = t >> 5, lane = t & 31, gq = lane >> 2, tq = lane & 3;
+    float *out = partial + (size_t)blockIdx.x * KP * NP;
+    for (int mt = warp; mt < KP / 16; mt += 4) {
+#pragma unroll
+        for (int nt = 0; nt < NP / 8; ++nt) {
+            float d[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 1
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int ks = 0; ks < kTile / 16; ++ks) {
+                    const __nv_bfloat16 *A0 = Tt + (a * KP + mt * 16 + gq) * RS + ks * 16 + 2 * tq;
+                    const __nv_bfloat16 *A1 = A0 + 8 * RS;
+                    const uint32_t a0 = *reinterpret_cast<const uint32_t *>(A0);
+                    const uint32_t a1 = *reinterpret_cast<const uint32_t *>(A1);
+                    const uint32_t a2 = *reinterpret_cast<const uint32_t *>(A0 + 8);
+                    const uint32_t a3 = *reinterpret_cast<const uint32_t *>(A1 + 8);
+                    const __nv_bfloat16 *B0 = Gt + (a * NP + nt * 8 + gq) * RS + ks * 16 + 2 * tq;
+                    const uint32_t b0 = *reinterpret_cast<const uint32_t *>(B0);
+                    const uint32_t b1 = *reinterpret_cast<const uint32_t *>(B0 + 8);
+                    mma_bf16(d, a0, a1, a2, a3, b0, b1);
+                }
+            const int k0 = mt * 16 + gq, n0 = nt * 8 + 2 * tq;
+            out[k0 * NP + n0] = d[0];
+            out[k0 * NP + n0 + 1] = d[1];
+            out[(k0 + 8) * NP + n0] = d[2];
+            out[(k0 + 8) * NP + n0 + 1] = d[3];
+        }
+    }
+}
+
+// fixed-order sum of the per-tile partials: dB[e] = sum_tile partial[tile][e]
+__global__ void ptc_reduce_kernel(const float *__restrict__ partial, int ntiles, int nelem, float *__restrict__ dB)
+{
+    __shared__ double sm[32];
+    for (int e = blockIdx.x; e < nelem; e += gridDim.x) {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < ntiles; b += blockDim.x) s += partial[(size_t)b * nelem + e];
+        s = block_sum(s, sm);
+        if (threadIdx.x == 0) dB[e] = (float)s;
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------- glue kernels
+// embed an FP64 parity field into channel 0 of a full-lattice activation (other parity zero)
+__global__ void ptc_embed_kernel(int vh, int pv, const void *__restrict__ src, int parity, float2 *__restrict__ act,
+                                 double scale)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= vh) return;
+    double v[6];
+    ld_spinor<0>(src, pv, i, v);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        act[(size_t)(parity * 3 + a) * pv + i] = make_float2((float)(scale * v[2 * a]), (float)(scale * v[2 * a + 1]));
+        act[(size_t)((1 - parity) * 3 + a) * pv + i] = make_float2(0.f, 0.f);
+    }
+}
+
+// channel 0, parity `parity` of an activation -> FP64 parity field (times scale)
+__global__ void ptc_extract_kernel(int vh, int pv, const float2 *__restrict__ act, int parity, void *__restrict__ dst,
+                                   double scale)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= vh) return;
+    double v[6];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float2 w = act[(size_t)(parity * 3 + a) * pv + i];
+        v[2 * a] = scale * w.x;
+        v[2 * a + 1] = scale * w.y;
+    }
+    st_spinor<0>(dst, pv, i, v);
+}
+
+// loss and output gradient of one pair: L = |y - e|^2 / |e|^2 on the parity sites; G = 2 (y - e) / |e|^2 there,
+// zero on the other parity.  y = channel 0 of the last activation; e an FP64 parity field.
+__global__ void ptc_loss_kernel(int vh, int pv, const float2 *__restrict__ y, const void *__restrict__ e, int parity,
+                                double inv_e2, float2 *__restrict__ gout, double *partials)
+{
+    __shared__ double sm[32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double l = 0.0;
+    if (i < vh) {
+        double ev[6];
+        ld_spinor<0>(e, pv, i, ev);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float2 w = y[(size_t)(parity * 3 + a) * pv + i];
+            const double dr = w.x - ev[2 * a], di = w.y - ev[2 * a + 1];
+            l += dr * dr + di * di;
+            gout[(size_t)(parity * 3 + a) * pv + i] = make_float2((float)(2 * dr * inv_e2), (float)(2 * di * inv_e2));
+            gout[(size_t)((1 - parity) * 3 + a) * pv + i] = make_float2(0.f, 0.f);
+        }
+    }
+    l = block_sum(l * inv_e2, sm);
+    if (threadIdx.x == 0) partials[blockIdx.x] = l;
+}
+
+// Adam on the real and imaginary parts of all weights
+__global__ void ptc_adam_kernel(float *w, const float *grad, float *m, float *v, int n, float lr, float b1, float b2,
+                                float eps, int step)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float gk = grad[k];
+    m[k] = b1 * m[k] + (1 - b1) * gk;
+    v[k] = b2 * v[k] + (1 - b2) * gk * gk;
+    const float mh = m[k] / (1 - powf(b1, (float)step)), vh = v[k] / (1 - powf(b2, (float)step));
+    w[k] -= lr * mh / (sqrtf(vh) + eps);
+}
+
+// ---------------------------------------------------------------------------------------------------- host side
+template <int CIN, int COUT>
+static size_t fwd_smem() { return (size_t)(3 * kTile + npad_of(COUT)) * (kpad_of(CIN) + 8) * 2; }
+template <int CIN, int COUT>
+static size_t wgrad_smem() { return (size_t)3 * (kpad_of(CIN) + npad_of(COUT)) * (kTile + 8) * 2; }
+
+template <int CIN, int COUT>
+static cudaError_t run_forward(const Geom &g, const LinkSet &fat, const float2 *in, float2 *out,
+                               const __nv_bfloat16 *Bt, bool swap, cudaStream_t s)
+{
+    const int pv = pad_sites(g.vh);
+    const int tiles = 2 * ((g.vh + kTile - 1) / kTile);
+    const size_t sm = fwd_smem<CIN, COUT>();
+    KQ_CUDA_TRY(cudaFuncSetAttribute(ptc_forward_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sm));
+    ptc_forward_kernel<CIN, COUT><<<tiles, kThr, sm, s>>>(g, pv, fat, in, out, Bt, swap ? 1 : 0);
+    return cudaGetLastError();
+}
+
+template <int CIN, int COUT>
+static cudaError_t run_wgrad(const Geom &g, const LinkSet &fat, const float2 *in, const float2 *gout, float *partial,
+                             float *dB, cudaStream_t s)
+{
+    const int pv = pad_sites(g.vh);
+    const int tiles = 2 * ((g.vh + kTile - 1) / kTile);
+    const size_t sm = wgrad_smem<CIN, COUT>();
+    KQ_CUDA_TRY(cudaFuncSetAttribute(ptc_wgrad_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sm));
+    ptc_wgrad_kernel<CIN, COUT><<<tiles, kThr, sm, s>>>(g, pv, fat, in, gout, partial);
+    const int nelem = kpad_of(CIN) * npad_of(COUT);
+    ptc_reduce_kernel<<<std::min(nelem, 1024), 256, 0, s>>>(partial, tiles, nelem, dB);
+    return cudaGetLastError();
+}
+
+cudaError_t ptc_forward(const Geom &g, const LinkSet &fat, int cin, int cout, const float2 *in, float2 *out,
+                        const void *Bt, bool swap, cudaStream_t s)
+{
+    const __nv_bfloat16 *B = static_cast<const __nv_bfloat16 *>(Bt);
+    if (cin == 1 && cout == 8) return run_forward<1, 8>(g, fat, in, out, B, swap, s);
+    if (cin == 8 && cout == 8) return run_forward<8, 8>(g, fat, in, out, B, swap, s);
+    if (cin == 8 && cout == 1) return run_forward<8, 1>(g, fat, in, out, B, swap, s);
+    if (cin == 1 && cout == 1) return run_forward<1, 1>(g, fat, in, out, B, swap, s);
+    set_last_error("ptc: channel counts must be 1 or 8");
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t ptc_wgrad(const Geom &g, const LinkSet &fat, int cin, int cout, const float2 *in, const float2 *gout,
+                      float *partial, float *dB, cudaStream_t s)
+{
+    if (cin == 1 && cout == 8) return run_wgrad<1, 8>(g, fat, in, gout, partial, dB, s);
+    if (cin == 8 && cout == 8) return run_wgrad<8, 8>(g, fat, in, gout, partial, dB, s);
+    if (cin == 8 && cout == 1) return run_wgrad<8, 1>(g, fat, in, gout, partial, dB, s);
+    if (cin == 1 && cout == 1) return run_wgrad<1, 1>(g, fat, in, gout, partial, dB, s);
+    set_last_error("ptc: channel counts must be 1 or 8");
+    return cudaErrorInvalidValue;
+}
+
+int ptc_kpad(int cin) { return kpad_of(cin); }
+int ptc_npad(int cout) { return npad_of(cout); }
+int ptc_tiles(const Geom &g) { return 2 * ((g.vh + kTile - 1) / kTile); }
+
+cudaError_t ptc_embed(const Geom &g, const void *src, int parity, float2 *act, double scale, cudaStream_t s)
+{
+    ptc_embed_kernel<<<(g.vh + 255) / 256, 256, 0, s>>>(g.vh, pad_sites(g.vh), src, parity, act, scale);
+    return cudaGetLastError();
+}
+
+cudaError_t ptc_extract(const Geom &g, const float2 *act, int parity, void *dst, double scale, cudaStream_t s)
+{
+    ptc_extract_kernel<<<(g.vh + 255) / 256, 256, 0, s>>>(g.vh, pad_sites(g.vh), act, parity, dst, scale);
+    return cudaGetLastError();
+}
+
+cudaError_t ptc_loss(const Geom &g, const float2 *y, const void *e, int parity, double inv_e2, float2 *gout,
+                     double *partials, double *loss_host, cudaStream_t s)
+{
+    const int nb = (g.vh + 255) / 256;
+    ptc_loss_kernel<<<nb, 256, 0, s>>>(g.vh, pad_sites(g.vh), y, e, parity, inv_e2, gout, partials);
+    KQ_CUDA_TRY(cudaGetLastError());
+    if (loss_host) {
+        std::vector<double> h(nb);
+        KQ_CUDA_TRY(cudaMemcpyAsync(h.data(), partials, sizeof(double) * nb, cudaMemcpyDeviceToHost, s));
+        KQ_CUDA_TRY(cudaStreamSynchronize(s));
+        double l = 0;
+        for (double v : h) l += v;
+        *loss_host = l;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t ptc_adam(float *w, const float *grad, float *m, float *v, int n, float lr, int step, cudaStream_t s)
+{
+    ptc_adam_kernel<<<(n + 255) / 256, 256, 0, s>>>(w, grad, m, v, n, lr, 0.9f, 0.999f, 1e-8f, step);
+    return cudaGetLastError();
+}
+
+}  // namespace kq

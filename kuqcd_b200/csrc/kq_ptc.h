@@ -1,0 +1,25 @@
+// Parallel-transport convolution layers (kq_ptc.cu) used by the learned preconditioner (kq_net.cu).
+#pragma once
+#include "kq_internal.h"
+
+namespace kq {
+
+// One layer, cin -> cout channels (1 or 8), on full-lattice activations (layout in kq_ptc.cu).  Bt: [npad][kpad]
+// BF16 GEMM matrix built from the complex weights.  swap = true gathers the hops with swapped path labels (the
+// adjoint layer, with conjugate-transposed weights).
+cudaError_t ptc_forward(const Geom &g, const LinkSet &fat, int cin, int cout, const float2 *in, float2 *out,
+                        const void *Bt, bool swap, cudaStream_t s);
+// dB[kpad][npad] = sum over all rows of T^T G  (T: the gathered inputs of `in`, G: the output gradient)
+cudaError_t ptc_wgrad(const Geom &g, const LinkSet &fat, int cin, int cout, const float2 *in, const float2 *gout,
+                      float *partial, float *dB, cudaStream_t s);
+int ptc_kpad(int cin);
+int ptc_npad(int cout);
+int ptc_tiles(const Geom &g);
+
+cudaError_t ptc_embed(const Geom &g, const void *src, int parity, float2 *act, double scale, cudaStream_t s);
+cudaError_t ptc_extract(const Geom &g, const float2 *act, int parity, void *dst, double scale, cudaStream_t s);
+cudaError_t ptc_loss(const Geom &g, const float2 *y, const void *e, int parity, double inv_e2, float2 *gout,
+                     double *partials, double *loss_host, cudaStream_t s);
+cudaError_t ptc_adam(float *w, const float *grad, float *m, float *v, int n, float lr, int step, cudaStream_t s);
+
+}  // namespace kq

@@ -65,7 +65,9 @@ EXPORTED_SYMBOLS = [
     "kq_mdagm_noalloc",
     "kq_solve_multishift", "kq_solve_multishift_device", "kq_true_residuals", "kq_make_links_record",
     "kq_make_source_record", "kq_last_error", "kq_batch_create", "kq_batch_destroy", "kq_batch_add",
-    "kq_batch_size", "kq_batch_solve", "kq_batch_system_info",
+    "kq_batch_size", "kq_batch_solve", "kq_batch_system_info", "kq_net_create", "kq_net_destroy",
+    "kq_net_num_weights", "kq_net_set_weights", "kq_net_get_weights", "kq_net_get_grad", "kq_net_zero_grad",
+    "kq_net_set_context", "kq_net_apply", "kq_net_train_pair", "kq_net_adam", "kq_fcg_polish",
 ]
 
 
@@ -124,6 +126,18 @@ def library() -> C.CDLL:
         "kq_batch_size": (i, [vp]),
         "kq_batch_solve": (i, [vp, C.POINTER(BatchInfo)]),
         "kq_batch_system_info": (i, [vp, i, C.POINTER(SolveInfo)]),
+        "kq_net_create": (i, [vp, i, C.POINTER(i), C.POINTER(vp)]),
+        "kq_net_destroy": (None, [vp]),
+        "kq_net_num_weights": (sz, [vp]),
+        "kq_net_set_weights": (i, [vp, C.POINTER(C.c_float), sz]),
+        "kq_net_get_weights": (i, [vp, C.POINTER(C.c_float), sz]),
+        "kq_net_get_grad": (i, [vp, C.POINTER(C.c_float), sz]),
+        "kq_net_zero_grad": (i, [vp]),
+        "kq_net_set_context": (i, [vp, vp]),
+        "kq_net_apply": (i, [vp, vp, vp, i]),
+        "kq_net_train_pair": (i, [vp, vp, vp, i, d, C.POINTER(d)]),
+        "kq_net_adam": (i, [vp, C.c_float, C.c_float]),
+        "kq_fcg_polish": (i, [vp, vp, C.POINTER(SolveParam), vp, vp, C.POINTER(SolveInfo)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -328,3 +342,80 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class Net:
+    """kq_net: the gauge-covariant parallel-transport convolution preconditioner of a context's lattice."""
+
+    def __init__(self, ctx: Context, channels=(1, 8, 8, 8, 1)):
+        h = C.c_void_p()
+        ch = (C.c_int * len(channels))(*channels)
+        st = library().kq_net_create(ctx._h, len(channels) - 1, ch, C.byref(h))
+        if st != 0:
+            raise KuQCDError(st, "kq_net_create")
+        self._h = h
+        self.ctx = ctx
+        self.channels = tuple(channels)
+        self.nw = int(library().kq_net_num_weights(h))
+
+    def _chk(self, st, where):
+        if st != 0:
+            raise KuQCDError(st, where)
+
+    @property
+    def weights(self) -> np.ndarray:
+        w = np.empty(self.nw, dtype=np.float32)
+        self._chk(library().kq_net_get_weights(self._h, w.ctypes.data_as(C.POINTER(C.c_float)), self.nw), "get_w")
+        return w
+
+    @weights.setter
+    def weights(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        self._chk(library().kq_net_set_weights(self._h, w.ctypes.data_as(C.POINTER(C.c_float)), w.size), "set_w")
+
+    def grad(self) -> np.ndarray:
+        g = np.empty(self.nw, dtype=np.float32)
+        self._chk(library().kq_net_get_grad(self._h, g.ctypes.data_as(C.POINTER(C.c_float)), self.nw), "get_grad")
+        return g
+
+    def zero_grad(self):
+        self._chk(library().kq_net_zero_grad(self._h), "zero_grad")
+
+    def use_context(self, ctx: Context):
+        self._chk(library().kq_net_set_context(self._h, ctx._h), "kq_net_set_context")
+        self.ctx = ctx
+
+    def apply(self, d_in, d_out, parity: int):
+        self._chk(library().kq_net_apply(self._h, _ptr(d_in), _ptr(d_out), parity), "kq_net_apply")
+
+    def train_pair(self, d_r, d_e, parity: int, e_norm2: float) -> float:
+        loss = C.c_double()
+        self._chk(library().kq_net_train_pair(self._h, _ptr(d_r), _ptr(d_e), parity, e_norm2, C.byref(loss)),
+                  "kq_net_train_pair")
+        return loss.value
+
+    def adam(self, lr: float, grad_scale: float = 1.0):
+        self._chk(library().kq_net_adam(self._h, lr, grad_scale), "kq_net_adam")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library().kq_net_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def fcg_polish(ctx: Context, net, d_b, d_x, shifts, parity=0, rel_residual=1e-10, max_iter=100000) -> SolveInfo:
+    """kq_fcg_polish: drive every shift of d_x (initial guesses) to the FP64 true-residual target; net=None: CG."""
+    p, keep = Context._param(shifts, parity, KQ_SOLVER_MIXED, KUQCD_DOUBLE, KUQCD_DOUBLE, max_iter, 0.0,
+                             rel_residual, 1)
+    info = SolveInfo()
+    st = library().kq_fcg_polish(ctx._h, net._h if net is not None else None, C.byref(p), _ptr(d_b), _ptr(d_x),
+                                 C.byref(info))
+    if st != 0:
+        raise KuQCDError(st, "kq_fcg_polish")
+    return info

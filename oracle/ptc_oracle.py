@@ -1,0 +1,137 @@
+"""ORACLE / TEST INFRASTRUCTURE ONLY — numpy float64 restatement of the parallel-transport convolution network of
+the learned preconditioner (kuqcd_b200/csrc/kq_ptc.cu, kq_net.cu), with its gradients.  Used by tests as the
+checker of the GPU forward and backward kernels (and checked itself against finite differences).
+
+Fields are arrays of shape (C, 2, Vh, 3) complex: channel, parity, checkerboard index, colour.  Links: the fat
+links of the host record scaled by 1/2 (the device copy the CUDA kernels read).  Layer:
+
+    y_o(x) = sum_c sum_p W[o, c, p] (T_p v_c)(x),  p = 0: identity, 1+2mu: F_mu(x) v(x+mu),
+                                                   2+2mu: F_mu(x-mu)^dag v(x-mu)
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+class Lattice:
+    def __init__(self, dims, fat_record):
+        self.dims = tuple(dims)
+        nx, ny, nz, nt = dims
+        self.vh = nx * ny * nz * nt // 2
+        hx = nx // 2
+        i = np.arange(self.vh)
+        xcb = i % hx
+        r = i // hx
+        y = r % ny
+        r //= ny
+        z = r % nz
+        t = r // nz
+        self.fwd = np.zeros((2, 4, self.vh), dtype=np.int64)
+        self.bwd = np.zeros((2, 4, self.vh), dtype=np.int64)
+        for par in (0, 1):
+            x = 2 * xcb + ((y + z + t + par) & 1)
+            c = [x, y, z, t]
+            n = [nx, ny, nz, nt]
+            for mu in range(4):
+                for hop, tab in ((1, self.fwd), (-1, self.bwd)):
+                    d = list(c)
+                    d[mu] = (c[mu] + hop) % n[mu]
+                    tab[par, mu] = (d[0] >> 1) + hx * (d[1] + ny * (d[2] + nz * d[3]))
+        F = fat_record.reshape(2, self.vh, 4, 9, 2)
+        self.U = 0.5 * (F[..., 0] + 1j * F[..., 1]).reshape(2, self.vh, 4, 3, 3)  # [par, i, mu, row, col]
+
+    def transports(self, v):
+        """v: (2, Vh, 3) -> list of 9 transported fields (identity, fwd mu, bwd mu ...)."""
+        out = [v]
+        for mu in range(4):
+            f = np.empty_like(v)
+            b = np.empty_like(v)
+            for par in (0, 1):
+                q = 1 - par
+                vn = v[q][self.fwd[par, mu]]
+                f[par] = np.einsum("iab,ib->ia", self.U[par, :, mu], vn)
+                nb = self.bwd[par, mu]
+                ub = self.U[q][nb, mu]
+                b[par] = np.einsum("iba,ib->ia", ub.conj(), v[q][nb])
+            out += [f, b]
+        return out
+
+
+def layer(lat, W, v):
+    """W: (Cout, Cin, 9) complex; v: (Cin, 2, Vh, 3)."""
+    y = np.zeros((W.shape[0],) + v.shape[1:], dtype=complex)
+    for c in range(W.shape[1]):
+        ts = lat.transports(v[c])
+        for p in range(9):
+            y += W[:, c, p][:, None, None, None] * ts[p][None]
+    return y
+
+
+def layer_adjoint(lat, W, g):
+    """Adjoint of `layer`: T_fwd^dag = T_bwd and vice versa, weights conjugate-transposed."""
+    swap = [0, 2, 1, 4, 3, 6, 5, 8, 7]
+    out = np.zeros((W.shape[1],) + g.shape[1:], dtype=complex)
+    for o in range(W.shape[0]):
+        ts = lat.transports(g[o])
+        for p in range(9):
+            out += np.conj(W[o, :, p])[:, None, None, None] * ts[swap[p]][None]
+    return out
+
+
+def embed(r, parity, vh):
+    v = np.zeros((1, 2, vh, 3), dtype=complex)
+    v[0, parity] = (r[0::2] + 1j * r[1::2]).reshape(vh, 3)
+    return v
+
+
+def extract(y, parity):
+    z = y[0, parity].reshape(-1)
+    out = np.empty(2 * z.size)
+    out[0::2], out[1::2] = z.real, z.imag
+    return out
+
+
+def weights_from_flat(flat, channels):
+    Ws, off = [], 0
+    for ci, co in zip(channels[:-1], channels[1:]):
+        n = co * ci * 9
+        w = flat[off:off + 2 * n]
+        Ws.append((w[0::2] + 1j * w[1::2]).reshape(co, ci, 9))
+        off += 2 * n
+    return Ws
+
+
+def flat_from_weights(Ws):
+    return np.concatenate([np.stack([W.real.ravel(), W.imag.ravel()], 1).ravel() for W in Ws])
+
+
+def apply(lat, Ws, r, parity):
+    v = embed(r, parity, lat.vh)
+    for W in Ws:
+        v = layer(lat, W, v)
+    return extract(v, parity)
+
+
+def loss_and_grad(lat, Ws, r, e, parity):
+    """L = |N(r) - e|^2 / |e|^2 and dL/dW (complex, re part = dL/dW_re, im part = dL/dW_im) per layer."""
+    acts = [embed(r, parity, lat.vh)]
+    for W in Ws:
+        acts.append(layer(lat, W, acts[-1]))
+    y = extract(acts[-1], parity)
+    e2 = float(e @ e)
+    L = float(((y - e) ** 2).sum()) / e2
+    d = 2 * (y - e) / e2
+    g = np.zeros_like(acts[-1])
+    g[0, parity] = (d[0::2] + 1j * d[1::2]).reshape(lat.vh, 3)
+    grads = [None] * len(Ws)
+    for li in range(len(Ws) - 1, -1, -1):
+        W = Ws[li]
+        dW = np.zeros_like(W)
+        for c in range(W.shape[1]):
+            ts = lat.transports(acts[li][c])
+            for p in range(9):
+                dW[:, c, p] = (g * np.conj(ts[p])[None]).sum(axis=(1, 2, 3))
+        grads[li] = dW
+        if li > 0:
+            g = layer_adjoint(lat, W, g)
+    return L, grads
