@@ -1,8 +1,8 @@
 // Per-shift flexible CG polish (FCG with one A-orthogonalisation, Notay's truncated FCG(1)) preconditioned by the
 // learned network: after a loose multishift pass, every shift's FP64 solution is driven to the true-residual
 // target with the FP64 operator (sigma_k + D^dag D).  Without a network, or when the preconditioned iteration
-// breaks down or exhausts its budget, the same loop continues unpreconditioned (plain CG from the current x): the
-// plain FP64 solver stays the fallback and the judge of the error.  No reference counterpart.
+// breaks down, stagnates or exhausts its budget, the same loop continues unpreconditioned (plain CG from the
+// current x), and every shift ends with an FP64 true-residual check.  No reference counterpart.
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -13,6 +13,7 @@
 
 struct kq_net;
 extern "C" KuQCDStatus kq_net_apply(kq_net *n, const void *d_in, void *d_out, int parity);
+int net_apply_launches(const kq_net *n);
 
 namespace kq {
 
@@ -149,7 +150,7 @@ KQ_API KuQCDStatus kq_fcg_polish(kq_context *ctx, kq_net *net, const kq_solve_pa
     void *r = c.take(vb), *z = c.take(vb), *p = c.take(vb), *w = c.take(vb), *tmp = c.take(vb), *s = c.take(vb);
     F.partials = static_cast<double *>(c.take(sizeof(double) * 3 * F.nb));
     const double target = param->rel_residual > 0 ? param->rel_residual : 1e-10;
-    const int max_iter = param->max_iter > 0 ? param->max_iter : 100000;
+    const int max_iter = param->max_iter > 0 ? param->max_iter : 20000;
     const int parity = param->parity;
     cudaStream_t st = ctx->stream;
     const int nb = F.nb, pv = F.pv;
@@ -171,7 +172,7 @@ KQ_API KuQCDStatus kq_fcg_polish(kq_context *ctx, kq_net *net, const kq_solve_pa
             if (F.err != cudaSuccess) return;
             if (use_net) {
                 if (kq_net_apply(net, in, out, parity) != KUQCD_SUCCESS) F.err = cudaErrorUnknown;
-                launches += 6;
+                launches += net_apply_launches(net);
             } else {
                 F.err = cudaMemcpyAsync(out, in, vb, cudaMemcpyDeviceToDevice, st);
             }
@@ -181,28 +182,40 @@ KQ_API KuQCDStatus kq_fcg_polish(kq_context *ctx, kq_net *net, const kq_solve_pa
         fcg_sub_kernel<<<nb, 256, 0, st>>>(g.vh, pv, d_b, s, r);
         double rr;
         F.dots(1, r, r, nullptr, nullptr, nullptr, nullptr, &rr);
+        // The network phase ends on convergence, on a breakdown (p^T A p <= 0), on stagnation (|r|^2 not halved over
+        // kStall iterations) or when its budget is spent; the unpreconditioned phase then starts from the current x
+        // with a budget of its own.  Every iteration of both phases counts in iter_refine.
+        constexpr int kStall = 200;
         bool use_net = net != nullptr;
-        int it = 0;
+        int it = 0;  // iterations of the current phase
         while (F.err == cudaSuccess && rr > target * target * bb && it < max_iter) {
             // (re)start: p = M r, w = A p
             precond(r, z, use_net);
             fcg_xpay_kernel<<<nb, 256, 0, st>>>(g.vh, pv, z, p, 0.0);
             matvec(p, w);
-            bool restart = false;
+            bool leave_net = false;
+            double rr_check = rr;
             while (F.err == cudaSuccess && it < max_iter) {
                 double d2[2];
                 F.dots(2, p, w, p, r, nullptr, nullptr, d2);  // pw, pr
                 const double pw = d2[0], alpha = d2[1] / pw;
                 if (!(pw > 0) || !std::isfinite(alpha)) {
-                    restart = use_net;  // breakdown: fall back to the unpreconditioned iteration
-                    use_net = false;
+                    leave_net = use_net;
                     break;
                 }
                 fcg_update_kernel<<<nb, 256, 0, st>>>(g.vh, pv, x, r, p, w, alpha);
                 ++it;
+                info->iter_refine += 1;
                 if (use_net) info->iter += 1;
                 F.dots(1, r, r, nullptr, nullptr, nullptr, nullptr, &rr);
                 if (rr <= target * target * bb) break;
+                if (use_net && it % kStall == 0) {
+                    if (!(rr < 0.5 * rr_check)) {
+                        leave_net = true;
+                        break;
+                    }
+                    rr_check = rr;
+                }
                 precond(r, z, use_net);
                 double zw;
                 F.dots(1, z, w, nullptr, nullptr, nullptr, nullptr, &zw);
@@ -210,22 +223,23 @@ KQ_API KuQCDStatus kq_fcg_polish(kq_context *ctx, kq_net *net, const kq_solve_pa
                 matvec(p, w);
                 launches += 5;
             }
-            if (!restart) {
-                if (F.err == cudaSuccess && rr > target * target * bb && use_net && it >= max_iter) {
-                    // budget exhausted with the network: one more budget without it
-                    use_net = false;
-                    it = 0;
-                    continue;
+            if (use_net && (leave_net || (rr > target * target * bb && it >= max_iter))) {
+                use_net = false;
+                it = 0;
+                if (F.err == cudaSuccess) {  // the breakdown may have left no update: recompute r = b - A x
+                    matvec(x, s);
+                    fcg_sub_kernel<<<nb, 256, 0, st>>>(g.vh, pv, d_b, s, r);
+                    F.dots(1, r, r, nullptr, nullptr, nullptr, nullptr, &rr);
                 }
-                break;
+                continue;
             }
+            break;
         }
         // final FP64 true residual
         matvec(x, s);
         fcg_sub_kernel<<<nb, 256, 0, st>>>(g.vh, pv, d_b, s, r);
         F.dots(1, r, r, nullptr, nullptr, nullptr, nullptr, &rr);
         info->true_residual[k] = std::sqrt(rr / bb);
-        info->iter_refine += it;
         if (rr > target * target * bb) info->status = KQ_STATUS_MAXITER;
     }
     info->kernel_launches = launches;

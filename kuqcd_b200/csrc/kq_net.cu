@@ -2,8 +2,12 @@
 // weights, activations, gradients and Adam state on the device, and the C ABI to train and apply it.
 //
 // Weights: per layer complex W[o][i][p] (o < C_out, i < C_in, p < 9), stored as interleaved (re, im) floats, layers
-// concatenated.  The network is linear in its input: N(r) = L_{n-1}(...L_0(embed(r))), read back on r's parity.
-// Training pairs (r, e): loss |N(r) - e|^2 / |e|^2, gradients by the adjoint layers (kq_ptc.cu).
+// concatenated.  The layers form a linear map N = L_{K-1} ... L_0 from one channel to C_K channels; the
+// preconditioner is its Gram operator
+//     M(r) = extract( L_0^dag ... L_{K-1}^dag L_{K-1} ... L_0 embed(r) )
+// read back on r's parity, symmetric positive semi-definite by construction (up to BF16 rounding), as a CG-type
+// outer iteration wants.  Training pairs (r, e): loss |M(r) - e|^2 / |e|^2; every layer's weights get two gradient
+// contributions, one through L_l and one through L_l^dag (kq_ptc.cu computes both with the same GEMM kernels).
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -43,30 +47,36 @@ __global__ void net_build_bt_kernel(const float *__restrict__ W, int cin, int co
     Bt[e] = __float2bfloat16_rn(v);
 }
 
-// grad[o][i][p] += dW from dB[k][n] (k = (i*9+p)*2+kr, n = o*2+nr)
-__global__ void net_accum_grad_kernel(const float *__restrict__ dB, int cin, int cout, int np, float *__restrict__ grad)
+// grad[o][i][p] += dL/dW from the GEMM gradient dB[k][n] of the layer (cin -> cout).  Forward layer: k =
+// (i*9+p)*2+kr, n = o*2+nr.  Adjoint layer (the GEMM runs cout -> cin with W' = conj(W)): k = (o*9+p)*2+kr,
+// n = i*2+nr, and dL/dW = conj(dL/dW').  np: the GEMM's padded column count.
+__global__ void net_accum_grad_kernel(const float *__restrict__ dB, int cin, int cout, int np, int adjoint,
+                                      float *__restrict__ grad)
 {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= cout * cin * 9) return;
     const int o = e / (cin * 9), rem = e - o * cin * 9, i = rem / 9, p = rem - i * 9;
-    const int k0 = (i * 9 + p) * 2, n0 = o * 2;
+    const int k0 = ((adjoint ? o : i) * 9 + p) * 2, n0 = (adjoint ? i : o) * 2;
     const float d00 = dB[k0 * np + n0], d01 = dB[k0 * np + n0 + 1];
     const float d10 = dB[(k0 + 1) * np + n0], d11 = dB[(k0 + 1) * np + n0 + 1];
-    grad[2 * e] += d00 + d11;      // d/dW_re
-    grad[2 * e + 1] += d01 - d10;  // d/dW_im
+    grad[2 * e] += d00 + d11;                                // d/dW_re
+    grad[2 * e + 1] += adjoint ? d10 - d01 : d01 - d10;      // d/dW_im
 }
 
 }  // namespace kq
 
 struct kq_net {
     kq_context *ctx = nullptr;
+    int dims[4] = {0, 0, 0, 0};  // lattice of the contexts the network may use
+    int device = 0;
     int nl = 0;
     std::vector<int> ch;     // nl + 1 channel counts
     std::vector<size_t> woff;  // float offsets of each layer's weights
     size_t nw = 0;           // floats
     float *w = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
     std::vector<void *> bt, bta;  // per-layer forward / adjoint BF16 matrices
-    std::vector<float2 *> act;    // nl + 1 activations
+    std::vector<float2 *> act;    // nl + 1 activations of the forward chain: a_0 = embed(r), a_{l+1} = L_l a_l
+    std::vector<float2 *> cact;   // adjoint chain c_l = L_l^dag c_{l+1}, l < nl (c_nl = a_nl)
     float2 *gbuf[2] = {nullptr, nullptr};
     float *partial = nullptr, *dB = nullptr;
     double *lpart = nullptr;
@@ -86,16 +96,16 @@ static void net_free(kq_net *n)
     for (void *p : n->bt) F(p);
     for (void *p : n->bta) F(p);
     for (float2 *p : n->act) F(p);
+    for (float2 *p : n->cact) F(p);
     F(n->gbuf[0]), F(n->gbuf[1]);
 }
 
 KQ_API void kq_net_destroy(kq_net *n)
 {
     if (!n) return;
-    if (n->ctx) {
-        cudaSetDevice(n->ctx->device);
-        cudaStreamSynchronize(n->ctx->stream);
-    }
+    // the context the network last used may already be gone: synchronise the device instead of its stream
+    cudaSetDevice(n->device);
+    cudaDeviceSynchronize();
     net_free(n);
     delete n;
 }
@@ -103,8 +113,8 @@ KQ_API void kq_net_destroy(kq_net *n)
 KQ_API KuQCDStatus kq_net_create(kq_context *ctx, int nlayers, const int *channels, kq_net **out)
 {
     if (!ctx || !channels || !out) return KUQCD_ERR_NULL_POINTER;
-    if (nlayers < 1 || nlayers > 16 || channels[0] != 1 || channels[nlayers] != 1) {
-        set_last_error("kq_net_create: 1..16 layers, one input and one output channel");
+    if (nlayers < 1 || nlayers > 16 || channels[0] != 1) {
+        set_last_error("kq_net_create: 1..16 layers and one input channel");
         return KUQCD_ERR_INVALID_PARAM;
     }
     for (int l = 0; l <= nlayers; ++l)
@@ -115,6 +125,8 @@ KQ_API KuQCDStatus kq_net_create(kq_context *ctx, int nlayers, const int *channe
     kq_net *n = new (std::nothrow) kq_net();
     if (!n) return KUQCD_ERR_NO_MEMORY;
     n->ctx = ctx;
+    for (int d = 0; d < 4; ++d) n->dims[d] = ctx->g.n[d];
+    n->device = ctx->device;
     n->nl = nlayers;
     n->ch.assign(channels, channels + nlayers + 1);
     for (int l = 0; l < nlayers; ++l) {
@@ -136,6 +148,8 @@ KQ_API KuQCDStatus kq_net_create(kq_context *ctx, int nlayers, const int *channe
     A((void **)&n->v, n->nw * 4);
     n->act.assign(nlayers + 1, nullptr);
     for (int l = 0; l <= nlayers; ++l) A((void **)&n->act[l], n->act_stride * n->ch[l] * sizeof(float2));
+    n->cact.assign(nlayers, nullptr);
+    for (int l = 0; l < nlayers; ++l) A((void **)&n->cact[l], n->act_stride * n->ch[l] * sizeof(float2));
     A((void **)&n->gbuf[0], n->act_stride * 8 * sizeof(float2));
     A((void **)&n->gbuf[1], n->act_stride * 8 * sizeof(float2));
     n->bt.assign(nlayers, nullptr);
@@ -146,6 +160,7 @@ KQ_API KuQCDStatus kq_net_create(kq_context *ctx, int nlayers, const int *channe
         A(&n->bt[l], (size_t)ptc_kpad(ci) * ptc_npad(co) * 2);
         A(&n->bta[l], (size_t)ptc_kpad(co) * ptc_npad(ci) * 2);
         maxkn = std::max(maxkn, (size_t)ptc_kpad(ci) * ptc_npad(co));
+        maxkn = std::max(maxkn, (size_t)ptc_kpad(co) * ptc_npad(ci));
     }
     A((void **)&n->partial, (size_t)ptc_tiles(g) * maxkn * 4);
     A((void **)&n->dB, maxkn * 4);
@@ -197,16 +212,17 @@ KQ_API KuQCDStatus kq_net_zero_grad(kq_net *n)
     return status_of(cudaMemsetAsync(n->g, 0, n->nw * 4, n->ctx->stream));
 }
 
-// use the links of another context (same lattice) from now on
+// use the links of another context (same lattice) from now on; the previous context may already be destroyed
 KQ_API KuQCDStatus kq_net_set_context(kq_net *n, kq_context *ctx)
 {
     if (!n || !ctx) return KUQCD_ERR_NULL_POINTER;
     for (int d = 0; d < 4; ++d)
-        if (ctx->g.n[d] != n->ctx->g.n[d] || ctx->device != n->ctx->device) {
+        if (ctx->g.n[d] != n->dims[d] || ctx->device != n->device) {
             set_last_error("kq_net_set_context: different lattice or device");
             return KUQCD_ERR_INVALID_PARAM;
         }
-    cudaStreamSynchronize(n->ctx->stream);
+    cudaSetDevice(n->device);
+    cudaDeviceSynchronize();
     n->ctx = ctx;
     return KUQCD_SUCCESS;
 }
@@ -229,14 +245,20 @@ cudaError_t ensure_bt(kq_net *n)
     return cudaGetLastError();
 }
 
+// a_0 = embed(d_in), a_{l+1} = L_l a_l, c_nl = a_nl, c_l = L_l^dag c_{l+1}; the result is c_0 (cact[0])
 cudaError_t forward(kq_net *n, const void *d_in, int parity, double in_scale)
 {
     kq_context *ctx = n->ctx;
+    const LinkSet &fat = ctx->gd.fat[P32];
     KQ_CUDA_TRY(ensure_bt(n));
     KQ_CUDA_TRY(ptc_embed(ctx->g, d_in, parity, n->act[0], in_scale, ctx->stream));
     for (int l = 0; l < n->nl; ++l)
-        KQ_CUDA_TRY(ptc_forward(ctx->g, ctx->gd.fat[P32], n->ch[l], n->ch[l + 1], n->act[l], n->act[l + 1],
-                                n->bt[l], false, ctx->stream));
+        KQ_CUDA_TRY(ptc_forward(ctx->g, fat, n->ch[l], n->ch[l + 1], n->act[l], n->act[l + 1], n->bt[l], false,
+                                ctx->stream));
+    for (int l = n->nl - 1; l >= 0; --l) {
+        const float2 *in = (l == n->nl - 1) ? n->act[n->nl] : n->cact[l + 1];
+        KQ_CUDA_TRY(ptc_forward(ctx->g, fat, n->ch[l + 1], n->ch[l], in, n->cact[l], n->bta[l], true, ctx->stream));
+    }
     return cudaSuccess;
 }
 
@@ -248,7 +270,10 @@ KuQCDStatus prepare(kq_net *n)
 
 }  // namespace
 
-// d_out = N(d_in) on `parity` (FP64 fields of the context's layout)
+// kernels one kq_net_apply launches once its BF16 matrices are built: embed, 2 x nl layers, extract
+int net_apply_launches(const kq_net *n) { return n ? 2 + 2 * n->nl : 0; }
+
+// d_out = M(d_in) on `parity` (FP64 fields of the context's layout)
 KQ_API KuQCDStatus kq_net_apply(kq_net *n, const void *d_in, void *d_out, int parity)
 {
     if (!n || !d_in || !d_out) return KUQCD_ERR_NULL_POINTER;
@@ -257,12 +282,12 @@ KQ_API KuQCDStatus kq_net_apply(kq_net *n, const void *d_in, void *d_out, int pa
     KuQCDStatus st = prepare(n);
     if (st != KUQCD_SUCCESS) return st;
     cudaError_t e = forward(n, d_in, parity, 1.0);
-    if (e == cudaSuccess) e = ptc_extract(n->ctx->g, n->act[n->nl], parity, d_out, 1.0, n->ctx->stream);
+    if (e == cudaSuccess) e = ptc_extract(n->ctx->g, n->cact[0], parity, d_out, 1.0, n->ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(n->ctx->stream);
     return status_of(e);
 }
 
-// forward + loss + backward for one pair (r, e); gradients are added to the accumulator.  loss: |N(r)-e|^2/|e|^2
+// forward + loss + backward for one pair (r, e); gradients are added to the accumulator.  loss: |M(r)-e|^2/|e|^2
 KQ_API KuQCDStatus kq_net_train_pair(kq_net *n, const void *d_r, const void *d_e, int parity, double e_norm2,
                                      double *loss)
 {
@@ -272,22 +297,36 @@ KQ_API KuQCDStatus kq_net_train_pair(kq_net *n, const void *d_r, const void *d_e
     KuQCDStatus st = prepare(n);
     if (st != KUQCD_SUCCESS) return st;
     kq_context *ctx = n->ctx;
+    const LinkSet &fat = ctx->gd.fat[P32];
     cudaStream_t s = ctx->stream;
     cudaError_t e = forward(n, d_r, parity, 1.0);
     double l = 0;
     int cur = 0;
-    if (e == cudaSuccess)
-        e = ptc_loss(ctx->g, n->act[n->nl], d_e, parity, 1.0 / e_norm2, n->gbuf[cur], n->lpart, &l, s);
+    if (e == cudaSuccess) e = ptc_loss(ctx->g, n->cact[0], d_e, parity, 1.0 / e_norm2, n->gbuf[cur], n->lpart, &l, s);
+    auto accum = [&](int layer, bool adjoint) {
+        if (e != cudaSuccess) return;
+        const int ci = n->ch[layer], co = n->ch[layer + 1];
+        net_accum_grad_kernel<<<(co * ci * 9 + 255) / 256, 256, 0, s>>>(
+            n->dB, ci, co, ptc_npad(adjoint ? ci : co), adjoint ? 1 : 0, n->g + n->woff[layer]);
+        e = cudaGetLastError();
+    };
+    // adjoint chain, output side first: gbuf[cur] holds dL/dc_l; c_l = L_l^dag c_{l+1} gives the adjoint-layer
+    // weight gradient and dL/dc_{l+1} = L_l dL/dc_l
+    for (int layer = 0; layer < n->nl && e == cudaSuccess; ++layer) {
+        const int ci = n->ch[layer], co = n->ch[layer + 1];
+        const float2 *in = (layer == n->nl - 1) ? n->act[n->nl] : n->cact[layer + 1];
+        e = ptc_wgrad(ctx->g, fat, co, ci, in, n->gbuf[cur], n->partial, n->dB, true, s);
+        accum(layer, true);
+        if (e == cudaSuccess) e = ptc_forward(ctx->g, fat, ci, co, n->gbuf[cur], n->gbuf[1 - cur], n->bt[layer], false, s);
+        cur = 1 - cur;
+    }
+    // forward chain: gbuf[cur] holds dL/da_{l+1}; dL/da_l = L_l^dag dL/da_{l+1}
     for (int layer = n->nl - 1; layer >= 0 && e == cudaSuccess; --layer) {
         const int ci = n->ch[layer], co = n->ch[layer + 1];
-        e = ptc_wgrad(ctx->g, ctx->gd.fat[P32], ci, co, n->act[layer], n->gbuf[cur], n->partial, n->dB, s);
-        if (e == cudaSuccess) {
-            net_accum_grad_kernel<<<(co * ci * 9 + 255) / 256, 256, 0, s>>>(n->dB, ci, co, ptc_npad(co),
-                                                                             n->g + n->woff[layer]);
-            e = cudaGetLastError();
-        }
+        e = ptc_wgrad(ctx->g, fat, ci, co, n->act[layer], n->gbuf[cur], n->partial, n->dB, false, s);
+        accum(layer, false);
         if (layer > 0 && e == cudaSuccess) {
-            e = ptc_forward(ctx->g, ctx->gd.fat[P32], co, ci, n->gbuf[cur], n->gbuf[1 - cur], n->bta[layer], true, s);
+            e = ptc_forward(ctx->g, fat, co, ci, n->gbuf[cur], n->gbuf[1 - cur], n->bta[layer], true, s);
             cur = 1 - cur;
         }
     }

@@ -176,9 +176,11 @@ __global__ void __launch_bounds__(kThr) ptc_forward_kernel(Geom g, int pv, LinkS
 
 // ---------------------------------------------------------------------------------------------------- weight grad
 // partial[tile][k][n] = sum over the tile's rows (sites x colours) of T[row][k] * G[row][n]
+// (swap_paths: T gathered as by the adjoint layer)
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(kThr) ptc_wgrad_kernel(Geom g, int pv, LinkSet fat, const float2 *__restrict__ in,
-                                                         const float2 *__restrict__ gout, float *__restrict__ partial)
+                                                         const float2 *__restrict__ gout, float *__restrict__ partial,
+                                                         int swap_paths)
 {
     constexpr int KP = kpad_of(CIN), NP = npad_of(COUT), RS = kTile + 8;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -192,7 +194,7 @@ __global__ void __launch_bounds__(kThr) ptc_wgrad_kernel(Geom g, int pv, LinkSet
     for (int a = 0; a < 3; ++a)
         for (int k = 0; k < KP; ++k) Tt[(a * KP + k) * RS + t] = __float2bfloat16_rn(0.f);
     if (i < g.vh) {
-        gather_site<CIN>(g, pv, fat, in, par, i, false, [&](int a, int k, float v) {
+        gather_site<CIN>(g, pv, fat, in, par, i, swap_paths != 0, [&](int a, int k, float v) {
             Tt[(a * KP + k) * RS + t] = __float2bfloat16_rn(v);
         });
     }
@@ -342,14 +344,14 @@ static cudaError_t run_forward(const Geom &g, const LinkSet &fat, const float2 *
 
 template <int CIN, int COUT>
 static cudaError_t run_wgrad(const Geom &g, const LinkSet &fat, const float2 *in, const float2 *gout, float *partial,
-                             float *dB, cudaStream_t s)
+                             float *dB, bool swap, cudaStream_t s)
 {
     const int pv = pad_sites(g.vh);
     const int tiles = 2 * ((g.vh + kTile - 1) / kTile);
     const size_t sm = wgrad_smem<CIN, COUT>();
     KQ_CUDA_TRY(cudaFuncSetAttribute(ptc_wgrad_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sm));
-    ptc_wgrad_kernel<CIN, COUT><<<tiles, kThr, sm, s>>>(g, pv, fat, in, gout, partial);
+    ptc_wgrad_kernel<CIN, COUT><<<tiles, kThr, sm, s>>>(g, pv, fat, in, gout, partial, swap ? 1 : 0);
     const int nelem = kpad_of(CIN) * npad_of(COUT);
     ptc_reduce_kernel<<<std::min(nelem, 1024), 256, 0, s>>>(partial, tiles, nelem, dB);
     return cudaGetLastError();
@@ -368,12 +370,12 @@ cudaError_t ptc_forward(const Geom &g, const LinkSet &fat, int cin, int cout, co
 }
 
 cudaError_t ptc_wgrad(const Geom &g, const LinkSet &fat, int cin, int cout, const float2 *in, const float2 *gout,
-                      float *partial, float *dB, cudaStream_t s)
+                      float *partial, float *dB, bool swap, cudaStream_t s)
 {
-    if (cin == 1 && cout == 8) return run_wgrad<1, 8>(g, fat, in, gout, partial, dB, s);
-    if (cin == 8 && cout == 8) return run_wgrad<8, 8>(g, fat, in, gout, partial, dB, s);
-    if (cin == 8 && cout == 1) return run_wgrad<8, 1>(g, fat, in, gout, partial, dB, s);
-    if (cin == 1 && cout == 1) return run_wgrad<1, 1>(g, fat, in, gout, partial, dB, s);
+    if (cin == 1 && cout == 8) return run_wgrad<1, 8>(g, fat, in, gout, partial, dB, swap, s);
+    if (cin == 8 && cout == 8) return run_wgrad<8, 8>(g, fat, in, gout, partial, dB, swap, s);
+    if (cin == 8 && cout == 1) return run_wgrad<8, 1>(g, fat, in, gout, partial, dB, swap, s);
+    if (cin == 1 && cout == 1) return run_wgrad<1, 1>(g, fat, in, gout, partial, dB, swap, s);
     set_last_error("ptc: channel counts must be 1 or 8");
     return cudaErrorInvalidValue;
 }

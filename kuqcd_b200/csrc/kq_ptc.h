@@ -9,9 +9,10 @@ namespace kq {
 // adjoint layer, with conjugate-transposed weights).
 cudaError_t ptc_forward(const Geom &g, const LinkSet &fat, int cin, int cout, const float2 *in, float2 *out,
                         const void *Bt, bool swap, cudaStream_t s);
-// dB[kpad][npad] = sum over all rows of T^T G  (T: the gathered inputs of `in`, G: the output gradient)
+// dB[kpad][npad] = sum over all rows of T^T G  (T: the gathered inputs of `in` -- with swapped path labels for an
+// adjoint layer -- and G: the output gradient)
 cudaError_t ptc_wgrad(const Geom &g, const LinkSet &fat, int cin, int cout, const float2 *in, const float2 *gout,
-                      float *partial, float *dB, cudaStream_t s);
+                      float *partial, float *dB, bool swap, cudaStream_t s);
 int ptc_kpad(int cin);
 int ptc_npad(int cout);
 int ptc_tiles(const Geom &g);

@@ -409,7 +409,7 @@ class Net:
             pass
 
 
-def fcg_polish(ctx: Context, net, d_b, d_x, shifts, parity=0, rel_residual=1e-10, max_iter=100000) -> SolveInfo:
+def fcg_polish(ctx: Context, net, d_b, d_x, shifts, parity=0, rel_residual=1e-10, max_iter=20000) -> SolveInfo:
     """kq_fcg_polish: drive every shift of d_x (initial guesses) to the FP64 true-residual target; net=None: CG."""
     p, keep = Context._param(shifts, parity, KQ_SOLVER_MIXED, KUQCD_DOUBLE, KUQCD_DOUBLE, max_iter, 0.0,
                              rel_residual, 1)

@@ -7,6 +7,9 @@ links of the host record scaled by 1/2 (the device copy the CUDA kernels read). 
 
     y_o(x) = sum_c sum_p W[o, c, p] (T_p v_c)(x),  p = 0: identity, 1+2mu: F_mu(x) v(x+mu),
                                                    2+2mu: F_mu(x-mu)^dag v(x-mu)
+
+and the preconditioner is the Gram operator M = P^T N^dag N P of the chain N = L_{K-1} ... L_0 (P: embedding of
+one parity into a one-channel full-lattice field).
 """
 from __future__ import annotations
 
@@ -105,33 +108,54 @@ def flat_from_weights(Ws):
     return np.concatenate([np.stack([W.real.ravel(), W.imag.ravel()], 1).ravel() for W in Ws])
 
 
-def apply(lat, Ws, r, parity):
-    v = embed(r, parity, lat.vh)
-    for W in Ws:
-        v = layer(lat, W, v)
-    return extract(v, parity)
-
-
-def loss_and_grad(lat, Ws, r, e, parity):
-    """L = |N(r) - e|^2 / |e|^2 and dL/dW (complex, re part = dL/dW_re, im part = dL/dW_im) per layer."""
+def _chains(lat, Ws, r, parity):
+    """Forward chain a_0 = embed(r), a_{l+1} = L_l a_l and adjoint chain c_K = a_K, c_l = L_l^dag c_{l+1}."""
     acts = [embed(r, parity, lat.vh)]
     for W in Ws:
         acts.append(layer(lat, W, acts[-1]))
-    y = extract(acts[-1], parity)
+    cs = [None] * len(Ws) + [acts[-1]]
+    for li in range(len(Ws) - 1, -1, -1):
+        cs[li] = layer_adjoint(lat, Ws[li], cs[li + 1])
+    return acts, cs
+
+
+def apply(lat, Ws, r, parity):
+    """M(r) = extract(N^dag N embed(r)), N = L_{K-1} ... L_0 (the Gram form kq_net.cu evaluates)."""
+    return extract(_chains(lat, Ws, r, parity)[1][0], parity)
+
+
+def _wgrad(lat, v, g, ncout, swap=False):
+    """sum over sites and colours of g_o * conj(T_p v_c): the complex gradient of a layer's weights W[o, c, p]
+    (swap: path labels of the adjoint layer)."""
+    order = [0, 2, 1, 4, 3, 6, 5, 8, 7] if swap else list(range(9))
+    dW = np.zeros((ncout, v.shape[0], 9), dtype=complex)
+    for c in range(v.shape[0]):
+        ts = lat.transports(v[c])
+        for p in range(9):
+            dW[:, c, p] = (g * np.conj(ts[order[p]])[None]).sum(axis=(1, 2, 3))
+    return dW
+
+
+def loss_and_grad(lat, Ws, r, e, parity):
+    """L = |M(r) - e|^2 / |e|^2 and dL/dW (complex, re part = dL/dW_re, im part = dL/dW_im) per layer; each layer
+    collects one term through L_l and one through L_l^dag (whose weights are conj(W)^T, hence the conj)."""
+    acts, cs = _chains(lat, Ws, r, parity)
+    y = extract(cs[0], parity)
     e2 = float(e @ e)
     L = float(((y - e) ** 2).sum()) / e2
     d = 2 * (y - e) / e2
-    g = np.zeros_like(acts[-1])
+    g = np.zeros_like(cs[0])
     g[0, parity] = (d[0::2] + 1j * d[1::2]).reshape(lat.vh, 3)
-    grads = [None] * len(Ws)
-    for li in range(len(Ws) - 1, -1, -1):
+    K = len(Ws)
+    grads = [np.zeros_like(W) for W in Ws]
+    for li in range(K):  # adjoint chain: g = dL/dc_li
         W = Ws[li]
-        dW = np.zeros_like(W)
-        for c in range(W.shape[1]):
-            ts = lat.transports(acts[li][c])
-            for p in range(9):
-                dW[:, c, p] = (g * np.conj(ts[p])[None]).sum(axis=(1, 2, 3))
-        grads[li] = dW
+        dWa = _wgrad(lat, cs[li + 1], g, W.shape[1], swap=True)  # [i, o, p] of the adjoint layer
+        grads[li] += np.conj(dWa.transpose(1, 0, 2))
+        g = layer(lat, W, g)
+    for li in range(K - 1, -1, -1):  # forward chain: g = dL/da_{li+1}
+        W = Ws[li]
+        grads[li] += _wgrad(lat, acts[li], g, W.shape[0])
         if li > 0:
             g = layer_adjoint(lat, W, g)
     return L, grads

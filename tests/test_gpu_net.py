@@ -10,7 +10,7 @@ from kuqcd_b200 import learned as LN
 from oracle import oracle as O
 from oracle import ptc_oracle as P
 
-CH = (1, 8, 8, 8, 1)
+CH = (1, 8, 8)  # N: 1 -> 8 -> 8 channels; M = N^dag N runs four layers
 
 
 def ctx_for(dims, eps, seed, mass_links=None):
@@ -42,6 +42,24 @@ def test_net_forward_matches_oracle(cuda, parity):
     want = P.apply(lat, P.weights_from_flat(w.astype(np.float64), CH), r, parity)
     # BF16 operands in four layers: a few parts in a thousand
     assert np.linalg.norm(got - want) <= 3e-2 * np.linalg.norm(want)
+
+
+@pytest.mark.gpu
+def test_net_apply_is_symmetric_positive(cuda):
+    """M = N^dag N: <u, M v> = <M u, v> up to BF16 rounding, and <v, M v> > 0."""
+    dims = (8, 4, 4, 4)
+    ctx, fat, lng = ctx_for(dims, 0.4, 5)
+    net = K.Net(ctx, CH)
+    net.weights = (0.3 * np.random.default_rng(2).standard_normal(net.nw)).astype(np.float32)
+    u, v = O.make_source(dims, 0, 21), O.make_source(dims, 0, 22)
+    du, dv, mu, mv = field(ctx), field(ctx), field(ctx), field(ctx)
+    ctx.upload(K.KUQCD_DOUBLE, u, du)
+    ctx.upload(K.KUQCD_DOUBLE, v, dv)
+    net.apply(du, mu, 0)
+    net.apply(dv, mv, 0)
+    Mu, Mv = ctx.download(K.KUQCD_DOUBLE, mu), ctx.download(K.KUQCD_DOUBLE, mv)
+    assert abs(u @ Mv - Mu @ v) <= 2e-2 * np.linalg.norm(Mu) * np.linalg.norm(v)
+    assert v @ Mv > 0 and u @ Mu > 0
 
 
 @pytest.mark.gpu
@@ -92,7 +110,8 @@ def test_fcg_polish_plain_cg_converges(cuda):
 @pytest.mark.gpu
 def test_trained_network_reduces_polish_iterations(cuda):
     """Train on solver-generated pairs from 3 gauge fields, evaluate on a held-out field: the FCG polish with the
-    network needs fewer iterations than the unpreconditioned polish from the same loose multishift solution."""
+    network (on the three smallest shifts) needs fewer iterations than the unpreconditioned polish from the same
+    loose multishift solution, and every shift still reaches the FP64 true-residual target."""
     dims = (8, 8, 8, 8)
     eps, mass = 0.45, 0.05
     sig0 = mass * mass + 1e-4
@@ -115,9 +134,10 @@ def test_trained_network_reduces_polish_iterations(cuda):
     dx1 = torch.zeros(6 * vb, dtype=torch.uint8, device="cuda")
     dx2 = torch.zeros(6 * vb, dtype=torch.uint8, device="cuda")
     _, plain = LN.solve_with_polish(ctx, None, db, dx1, sig)
-    _, learned = LN.solve_with_polish(ctx, net, db, dx2, sig)
+    _, learned = LN.solve_with_polish(ctx, net, db, dx2, sig, net_max_shift=0.01)
     assert plain.status == 0 and learned.status == 0
     for k, s in enumerate(sig):
         x = ctx.download(K.KUQCD_DOUBLE, dx2[k * vb:(k + 1) * vb])
         assert O.true_residual(dims, fat, lng, 0, s, b, x) <= 1.05e-10
+    assert learned.iter > 0
     assert learned.iter_refine < plain.iter_refine, (learned.iter_refine, plain.iter_refine)

@@ -1,12 +1,13 @@
 """CPU tests of the numpy restatement of the learned preconditioner (oracle/ptc_oracle.py): gauge covariance,
-adjointness of the backward layer, and gradients against finite differences."""
+adjointness of the backward layer, symmetry and positivity of the Gram operator, and gradients against finite
+differences."""
 import numpy as np
 
 from oracle import oracle as O
 from oracle import ptc_oracle as P
 
 DIMS = (4, 4, 2, 2)
-CH = [1, 8, 8, 8, 1]
+CH = [1, 8, 8]
 
 
 def setup(seed=0):
@@ -28,8 +29,19 @@ def test_layer_adjoint_is_adjoint():
     assert abs(lhs - rhs) < 1e-10 * abs(lhs)
 
 
+def test_gram_operator_is_symmetric_positive():
+    """M = P^T N^dag N P: <u, M v> = <M u, v> and <v, M v> > 0 in the real inner product of the solver's fields."""
+    lat, Ws, rng = setup()
+    for par in (0, 1):
+        u = O.make_source(DIMS, par, 11)
+        v = O.make_source(DIMS, par, 12)
+        Mu, Mv = P.apply(lat, Ws, u, par), P.apply(lat, Ws, v, par)
+        assert abs(u @ Mv - Mu @ v) < 1e-12 * np.linalg.norm(Mu) * np.linalg.norm(v)
+        assert v @ Mv > 0
+
+
 def test_gauge_covariance():
-    """N(Omega r) = Omega N(r) for a gauge transformation Omega(x) applied to links and fields."""
+    """M(Omega r) = Omega M(r) for a gauge transformation Omega(x) applied to links and fields."""
     lat, Ws, rng = setup()
     vh = lat.vh
     # random SU(3)-like unitary per site (QR of a Gaussian matrix)
