@@ -81,6 +81,16 @@ KuQCDStatus kq_mdagm(kq_context *ctx, int prec, double sigma, const void *d_src,
 KuQCDStatus kq_mdagm_noalloc(kq_context *ctx, int prec, double sigma, const void *d_src, void *d_dst, int parity,
                              void *stream);
 
+/* Full-lattice (non-preconditioned, KUQCD_HISQ_DIRAC) fields: the parity-0 field followed by the parity-1 field,
+ * each kq_spinor_bytes(ctx, prec) long (host records: even sites then odd sites, V*6 values).
+ * d_dst = D d_src on both parities in one launch.  Replaces DiracHISQ::Dslash with diracType KUQCD_HISQ_DIRAC on
+ * KUQCD_ALL fields (dirac_hisq.cpp:128-136 neighbour offsets, 418-424 site/link offsets). */
+KuQCDStatus kq_dslash_full(kq_context *ctx, int prec, const void *d_src, void *d_dst, void *stream);
+/* d_dst = sigma*d_src - D D d_src on full-lattice fields; d_tmp: one full-lattice field.  Replaces
+ * DiracHISQ::MdaggM (dirac_hisq.cpp:457-462) with KUQCD_HISQ_DIRAC followed by Axmy (spinor_field.cpp:130-144). */
+KuQCDStatus kq_mdagm_full(kq_context *ctx, int prec, double sigma, const void *d_src, void *d_dst, void *d_tmp,
+                          void *stream);
+
 /* ---------------------------------------------------------------- solver */
 enum {
     KQ_SOLVER_CGM = 0,        /* multishift CG with the reference's recurrences (CGM::Invert), FP64 or FP32 */
@@ -91,8 +101,14 @@ enum {
                                   KQ_SOLVER_CGM up to rounding, 4N -> (4N+8)/8 vector sweeps per iteration) */
 };
 
+enum { KQ_PARITY_FULL = 2 };
+
 typedef struct {
-    int parity;               /* 0: source and solutions on even sites (EVEN_EVEN), 1: odd (ODD_ODD) */
+    int parity;               /* 0: source and solutions on even sites (EVEN_EVEN), 1: odd (ODD_ODD),
+                                 KQ_PARITY_FULL: full-lattice fields (KUQCD_HISQ_DIRAC); sigma - D D is block
+                                 diagonal there, so each parity is solved on its own, to tol / 2 (the reference
+                                 rule over both parities) or to the share of rel_residual |b| that keeps the
+                                 full-lattice residual within target */
     int num_shift;            /* 1..64 */
     const double *shifts;     /* see shift_mode */
     int shift_mode;           /* 0: reference semantics, x_j solves (shifts[0] + shifts[j] - DD) for j >= 1
@@ -116,13 +132,16 @@ typedef struct {
     double sloppy_residual;   /* KQ_SOLVER_MIXED: largest true relative residual after the sloppy multishift */
 } kq_solve_info;
 
-/* Host b (num Vh*6 values of host_prec) -> host x[k].  Copies in, solves on the device, copies out. */
+/* Host b (Vh*6 values of host_prec; V*6 for KQ_PARITY_FULL) -> host x[k].  Copies in, solves on the device,
+ * copies out. */
 KuQCDStatus kq_solve_multishift(kq_context *ctx, const kq_solve_param *param, const void *host_b,
                                 void *const *host_x, kq_solve_info *info);
-/* Same with device fields in FP64 (d_b: one field; d_x: num_shift fields, kq_spinor_bytes(ctx, 8) apart). */
+/* Same with device fields in FP64 (d_b: one field; d_x: num_shift fields, kq_spinor_bytes(ctx, 8) apart; twice
+ * that for KQ_PARITY_FULL). */
 KuQCDStatus kq_solve_multishift_device(kq_context *ctx, const kq_solve_param *param, const void *d_b, void *d_x,
                                        kq_solve_info *info);
-/* FP64 true relative residuals |b - (sigma_k - DD) x_k| / |b| of device FP64 fields (absolute sigmas). */
+/* FP64 true relative residuals |b - (sigma_k - DD) x_k| / |b| of device FP64 fields (absolute sigmas; parity
+ * KQ_PARITY_FULL: full-lattice fields, norms over both parities). */
 KuQCDStatus kq_true_residuals(kq_context *ctx, int parity, int num_shift, const double *sigma, const void *d_b,
                               const void *d_x, double *out);
 
@@ -156,10 +175,11 @@ KuQCDStatus kq_batch_system_info(const kq_batch *b, int i, kq_solve_info *out);
 /* ---------------------------------------------------------------- learned preconditioner
  * A gauge-covariant parallel-transport convolution network (layers of y_o = sum_i,p W[o][i][p] T_p v_i with the
  * context's fat links as parallel transporters; BF16 tensor-core channel mixing, FP32 accumulation) trained on
- * solver-generated residual/error pairs, used by a per-shift flexible-CG polish.  No reference counterpart (the
- * reference's CGM is unpreconditioned, inverter_cgm.cpp:17-87). */
+ * solver-generated residual/error pairs, used by a per-shift flexible-CG polish.  The preconditioner is the Gram
+ * operator M = N^dag N of the layer chain N (symmetric positive semi-definite by construction).  No reference
+ * counterpart (the reference's CGM is unpreconditioned, inverter_cgm.cpp:17-87). */
 typedef struct kq_net kq_net;
-/* channels[0..nlayers]: 1, 8, ..., 8, 1 */
+/* channels[0..nlayers] of N: 1, then 1 or 8 each (M runs the 2 * nlayers layers of N and N^dag) */
 KuQCDStatus kq_net_create(kq_context *ctx, int nlayers, const int *channels, kq_net **out);
 void kq_net_destroy(kq_net *net);
 size_t kq_net_num_weights(const kq_net *net); /* floats: complex weights as (re, im) pairs, layers concatenated */
@@ -169,15 +189,16 @@ KuQCDStatus kq_net_get_grad(const kq_net *net, float *grad, size_t count);
 KuQCDStatus kq_net_zero_grad(kq_net *net);
 /* switch to the links of another context of the same lattice */
 KuQCDStatus kq_net_set_context(kq_net *net, kq_context *ctx);
-/* d_out = N(d_in), FP64 fields of parity `parity` */
+/* d_out = M(d_in), FP64 fields of parity `parity` */
 KuQCDStatus kq_net_apply(kq_net *net, const void *d_in, void *d_out, int parity);
-/* one training pair: forward, loss |N(r) - e|^2 / e_norm2, backward; the weight gradient is accumulated */
+/* one training pair: forward, loss |M(r) - e|^2 / e_norm2, backward; the weight gradient is accumulated */
 KuQCDStatus kq_net_train_pair(kq_net *net, const void *d_r, const void *d_e, int parity, double e_norm2,
                               double *loss);
 /* Adam step on the accumulated gradient times grad_scale; clears the accumulator */
 KuQCDStatus kq_net_adam(kq_net *net, float lr, float grad_scale);
 /* Polish every shift of d_x (initial guesses, num_shift FP64 fields) to the FP64 true relative residual
- * param->rel_residual with FCG preconditioned by net (NULL: plain CG, also the fallback on breakdown). */
+ * param->rel_residual with FCG preconditioned by net (NULL: plain CG, also the fallback on breakdown, stagnation
+ * or an exhausted budget).  info->iter_refine: all polish iterations; info->iter: those that applied the net. */
 KuQCDStatus kq_fcg_polish(kq_context *ctx, kq_net *net, const kq_solve_param *param, const void *d_b, void *d_x,
                           kq_solve_info *info);
 

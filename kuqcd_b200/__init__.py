@@ -15,7 +15,7 @@ from .lib import (  # noqa: F401
     KUQCD_BATCH_ORDER, KUQCD_EVEN_EVEN, KUQCD_ODD_ODD, KUQCD_FAT_LINK, KUQCD_LONG_LINK, KUQCD_WILSON_LINK,
     KUQCD_GAUGE_RECON_NO, KUQCD_GAUGE_RECON_12, KUQCD_GAUGE_RECON_U14, KUQCD_GAUGE_RECON_8,
     KUQCD_WILSON_DIRAC, KUQCD_WILSONPC_DIRAC, KUQCD_HISQ_DIRAC, KUQCD_HISQPC_DIRAC, KUQCD_CG, KUQCD_CGM,
-    KUQCD_XYZT_ORDER, KUQCD_TZYX_ORDER, KQ_SOLVER_CGM, KQ_SOLVER_MIXED, KQ_SOLVER_CGM_WINDOWED,
+    KUQCD_XYZT_ORDER, KUQCD_TZYX_ORDER, KQ_SOLVER_CGM, KQ_SOLVER_MIXED, KQ_SOLVER_CGM_WINDOWED, KQ_PARITY_FULL,
     KuQCDGaugeParam, KuQCDInvertParam, SolveParam, SolveInfo, EXPORTED_SYMBOLS,
     library, lib_path, kuqcd_init, kuqcd_load_gaugefield, kuqcd_solve_multishift, kuqcd_gauge_free, kuqcd_end,
     Context, KuQCDError, Batch, BatchInfo, Net, fcg_polish,

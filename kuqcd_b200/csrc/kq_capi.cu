@@ -1,5 +1,6 @@
 // C ABI of libkuqcd_b200.so: contexts, link loading, dslash, solver entry points and the C-linkage twins of the
 // reference's five exported calls (kuqcd.cpp:288-487).
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -25,6 +26,14 @@ cudaError_t launch_mdagm(const Geom &g, const GaugeDev &gd, int prec, double sig
 cudaError_t true_residuals(const Geom &g, const GaugeDev &gd, int parity, int ns, const double *sigma,
                            const void *d_b, const void *d_x, size_t xstride, void *d_tmp, void *d_s, double *partials,
                            double *out, cudaStream_t s);
+cudaError_t true_residuals_full(const Geom &g, const GaugeDev &gd, int ns, const double *sigma, const void *d_b,
+                                const void *d_x, size_t xstride, void *d_tmp, void *d_s, double *partials,
+                                double *out, cudaStream_t s);
+cudaError_t launch_dslash_full(const Geom &g, const GaugeDev &gd, int prec, const void *src, const void *pvec,
+                               void *dst, double sigma, cudaStream_t s);
+cudaError_t launch_mdagm_full(const Geom &g, const GaugeDev &gd, int prec, double sigma, const void *src, void *tmp,
+                              void *dst, cudaStream_t s);
+cudaError_t norm2_p64(const Geom &g, const void *v, double *partials, double *out, cudaStream_t s);
 
 }  // namespace kq
 
@@ -301,6 +310,37 @@ KQ_API KuQCDStatus kq_mdagm(kq_context *ctx, int prec, double sigma, const void 
     return status_of(launch_mdagm(ctx->g, ctx->gd, p, sigma, d_src, d_tmp, d_dst, parity, pick_stream(ctx, stream)));
 }
 
+static KuQCDStatus full_prep(kq_context *ctx, int prec, int *p)
+{
+    *p = prec_from_api(prec);
+    if (*p < 0) return KUQCD_ERR_INVALID_PARAM;
+    if (!ctx->gd.have[*p]) {
+        KuQCDStatus st = kq_prepare_links(ctx, prec);
+        if (st != KUQCD_SUCCESS) return st;
+    }
+    cudaSetDevice(ctx->device);
+    return KUQCD_SUCCESS;
+}
+
+KQ_API KuQCDStatus kq_dslash_full(kq_context *ctx, int prec, const void *d_src, void *d_dst, void *stream)
+{
+    if (!ctx || !d_src || !d_dst) return KUQCD_ERR_NULL_POINTER;
+    int p;
+    KuQCDStatus st = full_prep(ctx, prec, &p);
+    if (st != KUQCD_SUCCESS) return st;
+    return status_of(launch_dslash_full(ctx->g, ctx->gd, p, d_src, nullptr, d_dst, 0.0, pick_stream(ctx, stream)));
+}
+
+KQ_API KuQCDStatus kq_mdagm_full(kq_context *ctx, int prec, double sigma, const void *d_src, void *d_dst, void *d_tmp,
+                                 void *stream)
+{
+    if (!ctx || !d_src || !d_dst || !d_tmp) return KUQCD_ERR_NULL_POINTER;
+    int p;
+    KuQCDStatus st = full_prep(ctx, prec, &p);
+    if (st != KUQCD_SUCCESS) return st;
+    return status_of(launch_mdagm_full(ctx->g, ctx->gd, p, sigma, d_src, d_tmp, d_dst, pick_stream(ctx, stream)));
+}
+
 KQ_API KuQCDStatus kq_make_links_record(kq_context *ctx, double eps, uint64_t seed, double *d_fat, double *d_long)
 {
     if (!ctx || !d_fat || !d_long) return KUQCD_ERR_NULL_POINTER;
@@ -336,8 +376,8 @@ static KuQCDStatus check_solve_param(const kq_context *ctx, const kq_solve_param
         set_last_error("solve: num_shift must be in 1..64");
         return KUQCD_ERR_INVALID_PARAM;
     }
-    if (p->parity != 0 && p->parity != 1) {
-        set_last_error("solve: parity must be 0 or 1");
+    if (p->parity != 0 && p->parity != 1 && p->parity != KQ_PARITY_FULL) {
+        set_last_error("solve: parity must be 0, 1 or KQ_PARITY_FULL");
         return KUQCD_ERR_INVALID_PARAM;
     }
     if (!ctx->fat_loaded || !ctx->long_loaded) {
@@ -351,26 +391,35 @@ KQ_API KuQCDStatus kq_true_residuals(kq_context *ctx, int parity, int num_shift,
                                      const void *d_b, const void *d_x, double *out)
 {
     if (!ctx || !sigma || !d_b || !d_x || !out) return KUQCD_ERR_NULL_POINTER;
-    if (num_shift < 1 || num_shift > kMaxShift || (parity != 0 && parity != 1)) return KUQCD_ERR_INVALID_PARAM;
+    const bool full = parity == KQ_PARITY_FULL;
+    if (num_shift < 1 || num_shift > kMaxShift || (parity != 0 && parity != 1 && !full))
+        return KUQCD_ERR_INVALID_PARAM;
     if (!ctx->gd.have[P64]) {
         KuQCDStatus st = kq_prepare_links(ctx, KUQCD_DOUBLE);
         if (st != KUQCD_SUCCESS) return st;
     }
     cudaSetDevice(ctx->device);
-    const size_t vb = spinor_bytes(ctx->g, P64);
+    const size_t vb = spinor_bytes(ctx->g, P64) * (full ? 2 : 1);
     const int nb = (ctx->g.vh + 255) / 256;
     Carve c(nullptr);
     c.take(vb);
     c.take(vb);
-    c.take(sizeof(double) * 2 * nb);
+    c.take(sizeof(double) * 4 * nb);
     cudaError_t e = ensure_work(ctx, c.off);
     if (e != cudaSuccess) return status_of(e);
     Carve w(ctx->work);
     void *tmp = w.take(vb), *s = w.take(vb);
-    double *partials = static_cast<double *>(w.take(sizeof(double) * 2 * nb));
-    e = true_residuals(ctx->g, ctx->gd, parity, num_shift, sigma, d_b, d_x, vb, tmp, s, partials, out, ctx->stream);
+    double *partials = static_cast<double *>(w.take(sizeof(double) * 4 * nb));
+    if (full)
+        e = true_residuals_full(ctx->g, ctx->gd, num_shift, sigma, d_b, d_x, vb, tmp, s, partials, out, ctx->stream);
+    else
+        e = true_residuals(ctx->g, ctx->gd, parity, num_shift, sigma, d_b, d_x, vb, tmp, s, partials, out,
+                           ctx->stream);
     return status_of(e);
 }
+
+static KuQCDStatus solve_full(kq_context *ctx, const kq_solve_param *p, const void *d_b, void *d_x,
+                              kq_solve_info *info);
 
 KQ_API KuQCDStatus kq_solve_multishift_device(kq_context *ctx, const kq_solve_param *p, const void *d_b, void *d_x,
                                               kq_solve_info *info)
@@ -378,6 +427,7 @@ KQ_API KuQCDStatus kq_solve_multishift_device(kq_context *ctx, const kq_solve_pa
     KuQCDStatus st = check_solve_param(ctx, p);
     if (st != KUQCD_SUCCESS) return st;
     if (!d_b || !d_x) return KUQCD_ERR_NULL_POINTER;
+    if (p->parity == KQ_PARITY_FULL) return solve_full(ctx, p, d_b, d_x, info);
     cudaSetDevice(ctx->device);
     double sig[kMaxShift];
     absolute_shifts(p, sig);
@@ -481,6 +531,64 @@ KQ_API KuQCDStatus kq_solve_multishift_device(kq_context *ctx, const kq_solve_pa
     return info->status == KQ_STATUS_BREAKDOWN ? KUQCD_ERR_UNKNOWN_ERROR : KUQCD_SUCCESS;
 }
 
+// Full-lattice solve: sigma - D D has no even-odd coupling, so x = (x_e, x_o) with each half the solution of its
+// own parity system.  The reference's rule on the full residual, zeta^2 (|r_e|^2 + |r_o|^2) < tol, holds when each
+// half meets tol / 2; a relative target eps |b| holds when each half meets eps |b| / sqrt(2).  Each half is solved
+// into a contiguous scratch (the parity solvers take shift-contiguous fields) and copied into the strided halves.
+static KuQCDStatus solve_full(kq_context *ctx, const kq_solve_param *p, const void *d_b, void *d_x,
+                              kq_solve_info *info)
+{
+    cudaSetDevice(ctx->device);
+    const Geom &g = ctx->g;
+    const size_t vb = spinor_bytes(g, P64);
+    const int ns = p->num_shift;
+    kq_solve_info local;
+    if (!info) info = &local;
+    memset(info, 0, sizeof(*info));
+    info->num_shift = ns;
+    const int nb = (g.vh + 255) / 256;
+    void *scratch = nullptr;
+    cudaError_t e = cudaMallocAsync(&scratch, vb * ns + sizeof(double) * 2 * nb, ctx->stream);
+    if (e != cudaSuccess) return status_of(e);
+    double *partials = reinterpret_cast<double *>(static_cast<char *>(scratch) + vb * ns);
+    double bb[2] = {0, 0};
+    for (int par = 0; par < 2 && e == cudaSuccess; ++par)
+        e = norm2_p64(g, static_cast<const char *>(d_b) + par * vb, partials, &bb[par], ctx->stream);
+    const double bt = bb[0] + bb[1];
+    double rr[kMaxShift] = {0};
+    KuQCDStatus st = status_of(e);
+    for (int par = 0; par < 2 && st == KUQCD_SUCCESS; ++par) {
+        char *xh = static_cast<char *>(d_x) + par * vb;
+        if (!(bb[par] > 0)) {  // zero source half: zero solution half
+            e = cudaMemset2DAsync(xh, 2 * vb, 0, vb, ns, ctx->stream);
+            st = status_of(e);
+            continue;
+        }
+        kq_solve_param q = *p;
+        q.parity = par;
+        q.tol = p->tol / 2;
+        q.rel_residual = p->rel_residual * std::sqrt(bt / (2 * bb[par]));
+        kq_solve_info hi;
+        st = kq_solve_multishift_device(ctx, &q, static_cast<const char *>(d_b) + par * vb, scratch, &hi);
+        if (st != KUQCD_SUCCESS && st != KUQCD_ERR_UNKNOWN_ERROR) break;
+        e = cudaMemcpy2DAsync(xh, 2 * vb, scratch, vb, vb, ns, cudaMemcpyDeviceToDevice, ctx->stream);
+        if (e != cudaSuccess) st = status_of(e);
+        info->iter = std::max(info->iter, hi.iter);
+        info->iter_refine += hi.iter_refine;
+        info->status = std::max(info->status, hi.status);
+        info->seconds += hi.seconds;
+        info->kernel_launches += hi.kernel_launches + 1;
+        info->sloppy_residual = std::max(info->sloppy_residual, hi.sloppy_residual);
+        for (int k = 0; k < ns; ++k) rr[k] += hi.true_residual[k] * hi.true_residual[k] * bb[par];
+    }
+    for (int k = 0; k < ns; ++k) info->true_residual[k] = bt > 0 ? std::sqrt(rr[k] / bt) : 0.0;
+    cudaFreeAsync(scratch, ctx->stream);
+    cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+    if (st == KUQCD_SUCCESS && e2 != cudaSuccess) st = status_of(e2);
+    if (st == KUQCD_SUCCESS && info->status == KQ_STATUS_BREAKDOWN) st = KUQCD_ERR_UNKNOWN_ERROR;
+    return st;
+}
+
 KQ_API KuQCDStatus kq_solve_multishift(kq_context *ctx, const kq_solve_param *p, const void *host_b,
                                        void *const *host_x, kq_solve_info *info)
 {
@@ -495,21 +603,27 @@ KQ_API KuQCDStatus kq_solve_multishift(kq_context *ctx, const kq_solve_param *p,
         return KUQCD_ERR_INVALID_PARAM;
     }
     cudaSetDevice(ctx->device);
-    const size_t vb = spinor_bytes(ctx->g, P64);
+    const int halves = p->parity == KQ_PARITY_FULL ? 2 : 1;
+    const size_t vb = spinor_bytes(ctx->g, P64) * halves;  // one (full-lattice or parity) field
+    const size_t hvb = spinor_bytes(ctx->g, P64);            // one parity
+    const size_t hrec = (size_t)ctx->g.vh * 6 * (hp == P64 ? 8 : 4);  // one parity host record
     const size_t io = (size_t)vb * (1 + p->num_shift);
     void *io_buf = nullptr;
     // the device fields for b and x live outside the solver workspace
     cudaError_t e = cudaMallocAsync(&io_buf, io, ctx->stream);
     if (e != cudaSuccess) return status_of(e);
     void *d_b = io_buf, *d_x = static_cast<char *>(io_buf) + vb;
-    st = kq_spinor_upload(ctx, KUQCD_DOUBLE, host_b, p->host_prec, d_b, nullptr);
+    for (int h = 0; h < halves && st == KUQCD_SUCCESS; ++h)
+        st = kq_spinor_upload(ctx, KUQCD_DOUBLE, static_cast<const char *>(host_b) + h * hrec, p->host_prec,
+                              static_cast<char *>(d_b) + h * hvb, nullptr);
     if (st == KUQCD_SUCCESS) st = kq_solve_multishift_device(ctx, p, d_b, d_x, info);
     if (st == KUQCD_SUCCESS || st == KUQCD_ERR_UNKNOWN_ERROR)
-        for (int k = 0; k < p->num_shift; ++k) {
-            KuQCDStatus s2 = kq_spinor_download(ctx, KUQCD_DOUBLE, static_cast<char *>(d_x) + k * vb, host_x[k],
-                                                p->host_prec, nullptr);
-            if (s2 != KUQCD_SUCCESS) st = s2;
-        }
+        for (int k = 0; k < p->num_shift; ++k)
+            for (int h = 0; h < halves; ++h) {
+                KuQCDStatus s2 = kq_spinor_download(ctx, KUQCD_DOUBLE, static_cast<char *>(d_x) + k * vb + h * hvb,
+                                                    static_cast<char *>(host_x[k]) + h * hrec, p->host_prec, nullptr);
+                if (s2 != KUQCD_SUCCESS) st = s2;
+            }
     cudaFreeAsync(io_buf, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
     return st;

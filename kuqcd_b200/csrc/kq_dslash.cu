@@ -35,6 +35,30 @@ __global__ void __launch_bounds__(256) dslash_xmy_kernel(Geom g, int pv, LinkSet
     st_spinor<SP>(s, pv, i, acc);
 }
 
+// Full-lattice (non-preconditioned, KUQCD_HISQ_DIRAC) operator: a full field is the parity-0 field followed by the
+// parity-1 field, `half` bytes apart.  blockIdx.y = output parity p; the input is the other half.  dst = D src on
+// both parities in one launch (dirac_hisq.cpp:128-136, 418-424 with offseti = offsetg = 0), or, with pvec,
+// dst = sigma * pvec - D src (the second half of sigma - D D).
+template <int LP, int SP>
+__global__ void __launch_bounds__(256) dslash_full_kernel(Geom g, int pv, LinkSet fat, LinkSet lng,
+                                                          const char *__restrict__ src, const char *__restrict__ pvec,
+                                                          char *__restrict__ dst, size_t half, double sigma)
+{
+    using T = typename Acc2<LP, SP>::T;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.vh) return;
+    const int p = blockIdx.y;
+    T acc[6];
+    dslash_site2<LP, SP>(g, pv, fat, lng, src + (1 - p) * half, p, i, acc);
+    if (pvec) {
+        T pv6[6];
+        ld_spinor<SP>(pvec + p * half, pv, i, pv6);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) acc[k] = (T)sigma * pv6[k] - acc[k];
+    }
+    st_spinor<SP>(dst + p * half, pv, i, acc);
+}
+
 static bool pair_ok(int lp, int sp)
 {
     return (lp == sp) || (lp == P16 && sp == P32);
@@ -90,6 +114,34 @@ cudaError_t launch_mdagm(const Geom &g, const GaugeDev &gd, int prec, double sig
                          void *dst, int parity, cudaStream_t s)
 {
     return launch_mdagm2(g, gd, prec, prec, sigma, src, tmp, dst, parity, s);
+}
+
+// full-lattice fields (2 x spinor_bytes): dst = D src, or dst = sigma * pvec - D src when pvec != nullptr
+cudaError_t launch_dslash_full(const Geom &g, const GaugeDev &gd, int prec, const void *src, const void *pvec,
+                               void *dst, double sigma, cudaStream_t s)
+{
+    if (!gd.have[prec]) {
+        set_last_error("dslash: links not resident in the requested precision");
+        return cudaErrorInvalidValue;
+    }
+    const dim3 grid((g.vh + 255) / 256, 2);
+    const int pv = pad_sites(g.vh);
+    const size_t half = spinor_bytes(g, prec);
+    auto S = static_cast<const char *>(src);
+    auto Pv = static_cast<const char *>(pvec);
+    auto D = static_cast<char *>(dst);
+    KQ_DISPATCH_PAIR(prec, prec, (dslash_full_kernel<LP, SP><<<grid, 256, 0, s>>>(g, pv, gd.fat[prec], gd.lng[prec],
+                                                                                  S, Pv, D, half, sigma)));
+    return cudaGetLastError();
+}
+
+// dst = sigma src - D D src on full-lattice fields; tmp: one full-lattice field
+cudaError_t launch_mdagm_full(const Geom &g, const GaugeDev &gd, int prec, double sigma, const void *src, void *tmp,
+                              void *dst, cudaStream_t s)
+{
+    cudaError_t e = launch_dslash_full(g, gd, prec, src, nullptr, tmp, 0.0, s);
+    if (e != cudaSuccess) return e;
+    return launch_dslash_full(g, gd, prec, tmp, src, dst, sigma, s);
 }
 
 }  // namespace kq

@@ -32,6 +32,7 @@ KUQCD_GAUGE_RECON_NO, KUQCD_GAUGE_RECON_U14, KUQCD_GAUGE_RECON_12, KUQCD_GAUGE_R
 KUQCD_WILSON_DIRAC, KUQCD_WILSONPC_DIRAC, KUQCD_HISQ_DIRAC, KUQCD_HISQPC_DIRAC = 0, 1, 2, 3
 KUQCD_CG, KUQCD_CGM = 0, 1
 KQ_SOLVER_CGM, KQ_SOLVER_MIXED, KQ_SOLVER_CGM_WINDOWED = 0, 1, 2
+KQ_PARITY_FULL = 2  # full-lattice (KUQCD_HISQ_DIRAC) fields: parity 0 then parity 1
 
 
 class KuQCDGaugeParam(C.Structure):
@@ -62,7 +63,7 @@ EXPORTED_SYMBOLS = [
     "kq_kuqcd_init", "kq_kuqcd_load_gaugefield", "kq_kuqcd_solve_multishift", "kq_kuqcd_gauge_free",
     "kq_kuqcd_end", "kq_context_create", "kq_context_destroy", "kq_load_links", "kq_prepare_links",
     "kq_spinor_bytes", "kq_spinor_upload", "kq_spinor_download", "kq_spinor_convert", "kq_dslash", "kq_mdagm",
-    "kq_mdagm_noalloc",
+    "kq_mdagm_noalloc", "kq_dslash_full", "kq_mdagm_full",
     "kq_solve_multishift", "kq_solve_multishift_device", "kq_true_residuals", "kq_make_links_record",
     "kq_make_source_record", "kq_last_error", "kq_batch_create", "kq_batch_destroy", "kq_batch_add",
     "kq_batch_size", "kq_batch_solve", "kq_batch_system_info", "kq_net_create", "kq_net_destroy",
@@ -114,6 +115,8 @@ def library() -> C.CDLL:
         "kq_dslash": (i, [vp, i, vp, vp, i, vp]),
         "kq_mdagm": (i, [vp, i, d, vp, vp, vp, i, vp]),
         "kq_mdagm_noalloc": (i, [vp, i, d, vp, vp, i, vp]),
+        "kq_dslash_full": (i, [vp, i, vp, vp, vp]),
+        "kq_mdagm_full": (i, [vp, i, d, vp, vp, vp, vp]),
         "kq_solve_multishift": (i, [vp, C.POINTER(SolveParam), vp, C.POINTER(vp), C.POINTER(SolveInfo)]),
         "kq_solve_multishift_device": (i, [vp, C.POINTER(SolveParam), vp, vp, C.POINTER(SolveInfo)]),
         "kq_true_residuals": (i, [vp, i, i, C.POINTER(d), vp, vp, C.POINTER(d)]),
@@ -256,6 +259,27 @@ class Context:
         """kq_mdagm_noalloc: returns the status (callers test the rejection paths)."""
         return library().kq_mdagm_noalloc(self._h, prec, sigma, _ptr(src), _ptr(dst), parity, stream)
 
+    def upload_full(self, prec: int, host: np.ndarray, dev, stream=None):
+        """Full-lattice host record (even sites then odd sites, V*6 values) -> full-lattice device field."""
+        h = np.ascontiguousarray(host)
+        n = h.size // 2
+        vb = self.spinor_bytes(prec)
+        self.upload(prec, h[:n], dev[:vb], stream)
+        self.upload(prec, h[n:], dev[vb:2 * vb], stream)
+
+    def download_full(self, prec: int, dev, host_dtype=np.float64, stream=None) -> np.ndarray:
+        vb = self.spinor_bytes(prec)
+        return np.concatenate([self.download(prec, dev[:vb], host_dtype, stream),
+                               self.download(prec, dev[vb:2 * vb], host_dtype, stream)])
+
+    def dslash_full(self, prec: int, src, dst, stream=None):
+        """kq_dslash_full: D on full-lattice fields (both parities, one launch)."""
+        self._chk(library().kq_dslash_full(self._h, prec, _ptr(src), _ptr(dst), stream), "kq_dslash_full")
+
+    def mdagm_full(self, prec: int, sigma: float, src, dst, tmp, stream=None):
+        self._chk(library().kq_mdagm_full(self._h, prec, sigma, _ptr(src), _ptr(dst), _ptr(tmp), stream),
+                  "kq_mdagm_full")
+
     @staticmethod
     def _param(shifts, parity, solver, prec, host_prec, max_iter, tol, rel_residual, shift_mode):
         sh = (C.c_double * len(shifts))(*[float(s) for s in shifts])
@@ -347,7 +371,7 @@ class Batch:
 class Net:
     """kq_net: the gauge-covariant parallel-transport convolution preconditioner of a context's lattice."""
 
-    def __init__(self, ctx: Context, channels=(1, 8, 8, 8, 1)):
+    def __init__(self, ctx: Context, channels=(1, 8, 8)):
         h = C.c_void_p()
         ch = (C.c_int * len(channels))(*channels)
         st = library().kq_net_create(ctx._h, len(channels) - 1, ch, C.byref(h))

@@ -122,6 +122,16 @@ void kqo_dslash_d(const int dims[4], const double *fat, const double *lng, const
 void kqo_dslash_f(const int dims[4], const float *fat, const float *lng, const float *src, float *dst,
                   int dst_parity) KQO_DSLASH_BODY(float)
 
+/* The non-PC operator of dirac_hisq.cpp:409-455 with diracType KUQCD_HISQ_DIRAC on KUQCD_ALL fields: offseti =
+ * offsetg = 0 and the neighbour tables of dirac_hisq.cpp:128-136 point even sites at the odd half (index + Vh) and
+ * odd sites at the even half, so each half of dst is the even-odd dslash of the other half of src. */
+void kqo_dslash_full_d(const int dims[4], const double *fat, const double *lng, const double *src, double *dst)
+{
+    const long n = (long)dims[0] * dims[1] * dims[2] * dims[3] / 2 * 6;
+    kqo_dslash_d(dims, fat, lng, src + n, dst, 0);
+    kqo_dslash_d(dims, fat, lng, src, dst + n, 1);
+}
+
 void kqo_mdaggm_d(const int dims[4], const double *fat, const double *lng, const double *src, double *dst,
                   double *tmp, int parity)
 {

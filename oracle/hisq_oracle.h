@@ -26,6 +26,9 @@ void kqo_dslash_d(const int dims[4], const double *fat, const double *lng, const
                   int dst_parity);
 void kqo_dslash_f(const int dims[4], const float *fat, const float *lng, const float *src, float *dst,
                   int dst_parity);
+/* full lattice (KUQCD_HISQ_DIRAC, dirac_hisq.cpp:128-136, 418-424): src/dst hold even sites then odd sites
+ * (V*6 values); every output site gets D applied to the other parity half */
+void kqo_dslash_full_d(const int dims[4], const double *fat, const double *lng, const double *src, double *dst);
 /* dst = D_pq D_qp src  (MdaggM, dirac_hisq.cpp:457-462); tmp has Vh*6 entries */
 void kqo_mdaggm_d(const int dims[4], const double *fat, const double *lng, const double *src, double *dst,
                   double *tmp, int parity);

@@ -93,6 +93,13 @@ def dslash(dims, fat, lng, src, dst_parity):
     return out
 
 
+def dslash_full(dims, fat, lng, src):
+    """Non-PC dslash on a full-lattice field (even sites then odd sites)."""
+    out = np.zeros_like(src)
+    port().kqo_dslash_full_d(_dims(dims), _p(fat), _p(lng), _p(src), _p(out))
+    return out
+
+
 def mdagm(dims, fat, lng, src, parity):
     out, tmp = np.zeros_like(src), np.zeros_like(src)
     port().kqo_mdaggm_d(_dims(dims), _p(fat), _p(lng), _p(src), _p(out), _p(tmp), parity)
@@ -122,6 +129,21 @@ def ref_dslash(dims, fat, lng, src, dst_parity):
     out = np.zeros_like(src)
     f = ref().kqref_dslash_d if src.dtype == np.float64 else ref().kqref_dslash_f
     st = f((C.c_uint * 4)(*dims), _p(fat), _p(lng), _p(src), _p(out), dst_parity, 1)
+    assert st == 0
+    return out
+
+
+def ref_mdagm(dims, fat, lng, src, parity):
+    """D_pq D_qp of the reference (MdaggM, no sigma)."""
+    out = np.zeros_like(src)
+    st = ref().kqref_mdaggm_d((C.c_uint * 4)(*dims), _p(fat), _p(lng), _p(src), _p(out), parity, 1)
+    assert st == 0
+    return out
+
+
+def ref_dslash_full(dims, fat, lng, src):
+    out = np.zeros_like(src)
+    st = ref().kqref_dslash_full_d((C.c_uint * 4)(*dims), _p(fat), _p(lng), _p(src), _p(out))
     assert st == 0
     return out
 

@@ -16,6 +16,9 @@
  *   kqref_dslash_{d,f}     -> one DiracHISQ<T,1,NO,NO>::Dslash (dirac_hisq.cpp:409-455) on even-odd fields,
  *                             host arrays in the NORMAL_ORDER layout of kuqcd.cpp:103-169.
  *   kqref_mdaggm_d         -> DiracHISQ::MdaggM (dirac_hisq.cpp:457-462).
+ *   kqref_dslash_full_d    -> DiracHISQ<double,1,NO,NO>::Dslash with diracType KUQCD_HISQ_DIRAC on KUQCD_ALL
+ *                             fields (the non-preconditioned operator, dirac_hisq.cpp:128-136, 418-424); host
+ *                             arrays hold even sites then odd sites.
  */
 #include <cstring>
 #include <new>
@@ -105,9 +108,37 @@ int run_dslash(const unsigned *lat, const T *fat, const T *lng, const T *src, T 
     return 0;
 }
 
+/* One non-PC dslash on full-lattice reference objects (KUQCD_ALL spinors, KUQCD_HISQ_DIRAC). */
+int run_dslash_full(const unsigned *lat, const double *fat, const double *lng, const double *src, double *dst)
+{
+    std::array<unsigned short, 4> grid{1, 1, 1, 1};
+    Lattice sup(lat[0], lat[1], lat[2], lat[3]);
+    LattBase all(sup, grid, 0, KUQCD_NORMAL_ORDER, KUQCD_TZYX_ORDER, KUQCD_DOUBLE, KUQCD_ALL);
+    CommBase comm(all);
+    GaugeField<double, 1, KUQCD_GAUGE_RECON_NO> gf(all, comm), gl(all, comm);
+    scatter_gauge(gf, fat);
+    scatter_gauge(gl, lng);
+    SpinorField<double, 1, 1> in(all), out(all);
+    scatter_spinor(in, src);
+    DiracHISQ<double, 1, KUQCD_GAUGE_RECON_NO, KUQCD_GAUGE_RECON_NO> d(KUQCD_HISQ_DIRAC, gf, gl, 0, nullptr);
+    d.Dslash(in, out, false);
+    gather_spinor(out, dst);
+    return 0;
+}
+
 } // namespace
 
 extern "C" {
+
+__attribute__((visibility("default"))) int kqref_dslash_full_d(const unsigned *lat, const double *fat,
+                                                               const double *lng, const double *src, double *dst)
+{
+    try {
+        return run_dslash_full(lat, fat, lng, src, dst);
+    } catch (...) {
+        return -1;
+    }
+}
 
 __attribute__((visibility("default"))) void kqref_set_grid1()
 {
