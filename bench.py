@@ -36,6 +36,9 @@ METRIC = "HISQ dslash GFLOP/s + HBM GB/s; multishift CG time to 1e-10, mixed vs 
 REL_RES = 1e-10
 DSLASH_FLOPS = 1146          # per output site
 DSLASH_BYTES = {8: 2400, 4: 1200, 2: 608}   # compulsory bytes per output site: 16 links + 1 in + 1 out spinor
+# DRAM traffic of one FP64 dslash_kernel launch per output site, from ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum = 1.238 GB at 32^4, Vh = 524,288: profiles/dslash_fp64_32x32x32x32.txt), scaled by sites
+DSLASH_FP64_TRAFFIC_PER_SITE = 1.238e9 / 524288
 # Workloads.  "32": 32^4, eps 0.3, m 0.05, 12 shifts 1e-4..1 (the default).  "48": 48^3x96, eps 0.4, m 0.02,
 # 16 shifts 1e-5..1.  ref_iters: iterations the reference CGM (inverter_cgm.cpp:17-87) needs on the workload
 # (seed 1000, tol (1e-10)^2 |b|^2, reference-semantics shifts): for 32^4 counted by running oracle/ref_iterations.py
@@ -316,7 +319,10 @@ def run_ours(args):
             "e2e": {"value": world / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": Vh * 6 * 8,
                     "d2h_bytes_per_step": NSHIFT * Vh * 6 * 8},
             "roofline": {"bound": "hbm", "kernel": f"dslash_kernel<{dom}>", "achieved": achieved, "peak": peak,
-                         "peak_source": peak_note, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "peak_source": peak_note, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": DSLASH_FP64_TRAFFIC_PER_SITE * Vh,
+                         "traffic_source": "ncu DRAM bytes of one launch at 32^4, scaled by output sites",
+                         "algorithmic_bytes": DSLASH_BYTES[8] * Vh,
                          "bytes_per_site": DSLASH_BYTES[8 if dom == 'fp64' else 4]},
             "dslash": dsl,
             "cpu_baseline": cpu,

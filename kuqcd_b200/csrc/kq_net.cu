@@ -23,8 +23,8 @@ using namespace kq;
 
 namespace kq {
 
-// Bt[n][k] (BF16) of the real GEMM for one layer.  Forward: k = (i*9 + p)*2 + kr, n = o*2 + nr.  Adjoint: the layer
-// maps C_out -> C_in channels with W'[i][o][p] = conj(W[o][i][p]).
+// Bt[n][k] (BF16) of the real GEMM for one layer.  Forward: k = (p*C_in + i)*2 + kr, n = o*2 + nr.  Adjoint: the
+// layer maps C_out -> C_in channels with W'[i][o][p] = conj(W[o][i][p]).
 __global__ void net_build_bt_kernel(const float *__restrict__ W, int cin, int cout, int adjoint,
                                     __nv_bfloat16 *__restrict__ Bt, int kp, int np)
 {
@@ -35,7 +35,7 @@ __global__ void net_build_bt_kernel(const float *__restrict__ W, int cin, int co
     const int co = adjoint ? cin : cout;  // output channels of the GEMM
     float v = 0.f;
     if (k < ci * 18 && n < co * 2) {
-        const int a = k / 18, p = (k / 2) % 9, kr = k & 1;  // a: GEMM input channel
+        const int p = k / (2 * ci), a = (k >> 1) - p * ci, kr = k & 1;  // a: GEMM input channel
         const int b = n >> 1, nr = n & 1;                   // b: GEMM output channel
         // forward: W[o=b][i=a][p];  adjoint: W'[i=b][o=a][p] = conj(W[o=a][i=b][p])
         const int o = adjoint ? a : b, i = adjoint ? b : a;
@@ -48,7 +48,7 @@ __global__ void net_build_bt_kernel(const float *__restrict__ W, int cin, int co
 }
 
 // grad[o][i][p] += dL/dW from the GEMM gradient dB[k][n] of the layer (cin -> cout).  Forward layer: k =
-// (i*9+p)*2+kr, n = o*2+nr.  Adjoint layer (the GEMM runs cout -> cin with W' = conj(W)): k = (o*9+p)*2+kr,
+// (p*cin+i)*2+kr, n = o*2+nr.  Adjoint layer (the GEMM runs cout -> cin with W' = conj(W)): k = (p*cout+o)*2+kr,
 // n = i*2+nr, and dL/dW = conj(dL/dW').  np: the GEMM's padded column count.
 __global__ void net_accum_grad_kernel(const float *__restrict__ dB, int cin, int cout, int np, int adjoint,
                                       float *__restrict__ grad)
@@ -56,7 +56,7 @@ __global__ void net_accum_grad_kernel(const float *__restrict__ dB, int cin, int
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= cout * cin * 9) return;
     const int o = e / (cin * 9), rem = e - o * cin * 9, i = rem / 9, p = rem - i * 9;
-    const int k0 = ((adjoint ? o : i) * 9 + p) * 2, n0 = (adjoint ? i : o) * 2;
+    const int k0 = (p * (adjoint ? cout : cin) + (adjoint ? o : i)) * 2, n0 = (adjoint ? i : o) * 2;
     const float d00 = dB[k0 * np + n0], d01 = dB[k0 * np + n0 + 1];
     const float d10 = dB[(k0 + 1) * np + n0], d11 = dB[(k0 + 1) * np + n0 + 1];
     grad[2 * e] += d00 + d11;                                // d/dW_re
@@ -283,7 +283,8 @@ KQ_API KuQCDStatus kq_net_apply(kq_net *n, const void *d_in, void *d_out, int pa
     if (st != KUQCD_SUCCESS) return st;
     cudaError_t e = forward(n, d_in, parity, 1.0);
     if (e == cudaSuccess) e = ptc_extract(n->ctx->g, n->cact[0], parity, d_out, 1.0, n->ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(n->ctx->stream);
+    if (e == cudaSuccess) e = ptc_check_fault(n->ctx->stream);
+    if (e != cudaSuccess) set_last_error(std::string("kq_net_apply: ") + cudaGetErrorString(e));
     return status_of(e);
 }
 
@@ -330,7 +331,7 @@ KQ_API KuQCDStatus kq_net_train_pair(kq_net *n, const void *d_r, const void *d_e
             cur = 1 - cur;
         }
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = ptc_check_fault(s);
     if (loss) *loss = l;
     if (e != cudaSuccess) set_last_error(std::string("kq_net_train_pair: ") + cudaGetErrorString(e));
     return status_of(e);

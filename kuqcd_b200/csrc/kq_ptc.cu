@@ -8,11 +8,15 @@
 //   T_0 = 1,  T_{1+2mu} v (x) = F_mu(x) v(x+mu),  T_{2+2mu} v (x) = F_mu(x-mu)^dag v(x-mu)
 //
 // with the FP32 device fat links F (they carry the dslash's factor 1/2) and complex weights W.  Per tile of 128
-// sites of one parity the transported inputs are gathered in FP32, rounded to BF16 into shared memory, and the
-// channel mixing is a real GEMM per colour: [128 x K] x [K x N], K = C_in*9*2 (re, im), N = C_out*2, on the tensor
-// cores (mma.sync m16n8k16 BF16, FP32 accumulate).  The adjoint layer (for input gradients) is the same kernel with
-// weights W'[i][o][p'] = conj(W[o][i][p]) and forward/backward hops swapped.  The weight gradient dL/dB = T^T G is a
-// second tensor-core GEMM over the rows of each tile; per-tile partials are summed in a fixed order.
+// sites of one parity the transported inputs are gathered in FP32 and rounded to BF16 into shared memory; the
+// channel mixing is then a real GEMM per colour, [128 x K] x [K x N] with K = 9 paths x C_in x (re, im) in the
+// order k = (p * C_in + i) * 2 + reim and N = C_out * 2 (padded to 16).  Forward layers run it on the
+// fifth-generation tensor cores: one thread issues tcgen05.mma (BF16 operands in shared memory in the canonical
+// K-major layout, FP32 accumulators in tensor memory, M = 128, N = 16, K = 16 per instruction) for the three
+// colours, and the epilogue reads the accumulators back with tcgen05.ld, one site row per thread.  The adjoint layer
+// (for input gradients) is the same kernel with weights W'[i][o][p'] = conj(W[o][i][p]) and forward/backward hops
+// swapped.  The weight gradient dL/dB = T^T G is a second GEMM over the rows of each tile (mma.sync BF16, FP32
+// accumulate); per-tile partials are summed in a fixed order.
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -23,6 +27,7 @@
 #include "kq_context.h"
 #include "kq_dslash_core.cuh"
 #include "kq_ptc.h"
+#include "kq_umma.cuh"
 
 namespace kq {
 
@@ -54,25 +59,27 @@ __device__ __forceinline__ float2 ld_act(const float2 *act, int pv, int c, int p
     return __ldg(act + (size_t)((c * 2 + par) * 3 + a) * pv + i);
 }
 
-// Gather the transported inputs of site i (parity par) for all channels and paths and hand them, colour by colour,
-// to `put(colour, k, value)` with k = (c*9 + p)*2 + reim.
-template <int CIN, typename Put>
-__device__ __forceinline__ void gather_site(const Geom &g, int pv, const LinkSet &fat, const float2 *act, int par,
-                                            int i, bool swap_paths, Put put)
+// Gather the transported inputs of site i (parity par) path by path: emit(p, vals) with vals[a][2 c + reim] the
+// colour-a component of (T_p v_c)(x), i.e. GEMM columns k = p * 2 CIN + 2 c + reim.
+template <int CIN, typename Emit>
+__device__ __forceinline__ void gather_paths(const Geom &g, int pv, const LinkSet &fat, const float2 *act, int par,
+                                             int i, bool swap_paths, Emit emit)
 {
     const SiteCoord cd = site_coord(g, i, par);
     const int q = 1 - par;
     const void *fat_p = par ? fat.par[1] : fat.par[0];
     const void *fat_q = par ? fat.par[0] : fat.par[1];
+    float vals[3][2 * CIN];
     // identity path
 #pragma unroll
     for (int c = 0; c < CIN; ++c)
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             const float2 v = ld_act(act, pv, c, par, a, i);
-            put(a, (c * kPaths + 0) * 2 + 0, v.x);
-            put(a, (c * kPaths + 0) * 2 + 1, v.y);
+            vals[a][2 * c] = v.x;
+            vals[a][2 * c + 1] = v.y;
         }
+    emit(0, vals);
 #pragma unroll 1
     for (int dir = 0; dir < 4; ++dir) {
 #pragma unroll
@@ -100,78 +107,124 @@ __device__ __forceinline__ void gather_site(const Geom &g, int pv, const LinkSet
                 }
 #pragma unroll
                 for (int a = 0; a < 3; ++a) {
-                    put(a, (c * kPaths + p) * 2 + 0, o[2 * a]);
-                    put(a, (c * kPaths + p) * 2 + 1, o[2 * a + 1]);
+                    vals[a][2 * c] = o[2 * a];
+                    vals[a][2 * c + 1] = o[2 * a + 1];
                 }
             }
+            emit(p, vals);
         }
     }
 }
 
 // ---------------------------------------------------------------------------------------------------- forward
-// out (C_out channels, both parities) = layer(in); Bt: [N_pad][K_pad] BF16 weights (device), built by the host.
+// out (C_out channels, both parities) = layer(in); Bt: [NP][KP] BF16 weights (device), built by the host.
+// fault: set when the tensor cores did not signal completion within the wait limit (the tile is then not written).
+constexpr int kNT = 16;                      // N of the tensor-core tile (C_out * 2 padded)
+constexpr uint32_t kTmemCols = 64;           // 3 colours x 16 FP32 accumulator columns, rounded up
+constexpr uint32_t kWaitLimit = 1u << 24;    // mbarrier polls before a tile gives up
+
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(kThr) ptc_forward_kernel(Geom g, int pv, LinkSet fat, const float2 *__restrict__ in,
                                                            float2 *__restrict__ out, const __nv_bfloat16 *__restrict__ Bt,
-                                                           int swap_paths)
+                                                           int swap_paths, int *fault)
 {
-    constexpr int KP = kpad_of(CIN), NP = npad_of(COUT), KS = KP + 8;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __nv_bfloat16 *As = reinterpret_cast<__nv_bfloat16 *>(smem_raw);  // [3][kTile][KS]
-    __nv_bfloat16 *Bs = As + 3 * kTile * KS;                          // [NP][KS]
+    constexpr int KP = kpad_of(CIN), NP = npad_of(COUT), KV = CIN * kPaths * 2;
+    constexpr uint32_t A_BYTES = kTile * KP * 2;   // one colour's [128 x KP] operand
+    constexpr uint32_t SBO = (KP / 8) * 128;       // bytes between 8-row groups
+    static_assert(NP <= kNT && KP % 16 == 0, "tile shape");
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char *As = smem_raw;                  // [3][A_BYTES]
+    unsigned char *Bs = As + 3 * A_BYTES;          // [kNT x KP]
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(Bs + kNT * KP * 2);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
     const int tiles_per_par = (g.vh + kTile - 1) / kTile;
     const int par = blockIdx.x / tiles_per_par;
     const int base = (blockIdx.x - par * tiles_per_par) * kTile;
-    const int t = threadIdx.x;
-    for (int e = t; e < NP * KP; e += kThr) {
+    const int t = threadIdx.x, warp = t >> 5;
+    if (warp == 0) umma::tmem_alloc(tslot, kTmemCols);
+    if (t == 0) {
+        umma::mbar_init(mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int e = t; e < kNT * KP; e += kThr) {
         const int n = e / KP, k = e - n * KP;
-        Bs[n * KS + k] = Bt[e];
+        *reinterpret_cast<__nv_bfloat16 *>(Bs + umma::kmajor_offset(n, k, KP)) =
+            n < NP ? Bt[n * KP + k] : __float2bfloat16_rn(0.f);
     }
     const int i = base + t;
     if (i < g.vh) {
-        gather_site<CIN>(g, pv, fat, in, par, i, swap_paths != 0, [&](int a, int k, float v) {
-            As[(a * kTile + t) * KS + k] = __float2bfloat16_rn(v);
+        gather_paths<CIN>(g, pv, fat, in, par, i, swap_paths != 0, [&](int p, const float (&vals)[3][2 * CIN]) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                unsigned char *row = As + a * A_BYTES;
+                if constexpr (CIN == 8) {
+                    // 16 columns = two core-matrix rows of 16 bytes
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        uint4 w;
+                        w.x = pack_bf16(vals[a][8 * h + 0], vals[a][8 * h + 1]);
+                        w.y = pack_bf16(vals[a][8 * h + 2], vals[a][8 * h + 3]);
+                        w.z = pack_bf16(vals[a][8 * h + 4], vals[a][8 * h + 5]);
+                        w.w = pack_bf16(vals[a][8 * h + 6], vals[a][8 * h + 7]);
+                        *reinterpret_cast<uint4 *>(row + umma::kmajor_offset(t, p * 16 + 8 * h, KP)) = w;
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 2 * CIN; j += 2)
+                        *reinterpret_cast<uint32_t *>(row + umma::kmajor_offset(t, p * 2 * CIN + j, KP)) =
+                            pack_bf16(vals[a][j], vals[a][j + 1]);
+                }
+            }
         });
 #pragma unroll
         for (int a = 0; a < 3; ++a)
-            for (int k = CIN * kPaths * 2; k < KP; ++k) As[(a * kTile + t) * KS + k] = __float2bfloat16_rn(0.f);
+            for (int k = KV; k < KP; k += 2)
+                *reinterpret_cast<uint32_t *>(As + a * A_BYTES + umma::kmajor_offset(t, k, KP)) = 0u;
     } else {
+#pragma unroll
         for (int a = 0; a < 3; ++a)
-            for (int k = 0; k < KP; ++k) As[(a * kTile + t) * KS + k] = __float2bfloat16_rn(0.f);
+            for (int k = 0; k < KP; k += 8)
+                *reinterpret_cast<uint4 *>(As + a * A_BYTES + umma::kmajor_offset(t, k, KP)) = make_uint4(0, 0, 0, 0);
     }
+    umma::fence_smem_to_async();
+    umma::fence_before_sync();
     __syncthreads();
-    const int warp = t >> 5, lane = t & 31, gq = lane >> 2, tq = lane & 3;
+    umma::fence_after_sync();
+    const uint32_t tbase = *tslot;
+    if (t == 0) {
+        constexpr uint32_t idesc = umma::idesc_bf16_f32(kTile, kNT);
+        const uint32_t a0 = umma::smem_u32(As), b0 = umma::smem_u32(Bs);
 #pragma unroll 1
-    for (int a = 0; a < 3; ++a) {
+        for (int a = 0; a < 3; ++a)
 #pragma unroll
-        for (int mt = 0; mt < 2; ++mt) {
-            const int r0 = warp * 32 + mt * 16;
+            for (int ks = 0; ks < KP / 16; ++ks)
+                umma::mma_bf16(tbase + a * kNT, umma::smem_desc(a0 + a * A_BYTES + ks * 256, SBO),
+                               umma::smem_desc(b0 + ks * 256, SBO), idesc, ks > 0 ? 1u : 0u);
+        umma::mma_commit(mbar);
+    }
+    bool ok = umma::mbar_wait(mbar, 0, kWaitLimit);
+    ok = __syncthreads_and(ok);
+    if (!ok) {
+        if (t == 0) atomicExch(fault, 1);
+        umma::mbar_wait(mbar, 0, kWaitLimit);  // give the MMAs in flight a last chance before freeing their memory
+    }
+    umma::fence_after_sync();
+    if (ok) {
+        const int site = base + t;  // tensor-memory lane t = row t of the tile
+#pragma unroll 1
+        for (int a = 0; a < 3; ++a) {
+            float d[16];
+            umma::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + a * kNT, d);
+            if (site < g.vh) {
 #pragma unroll
-            for (int nt = 0; nt < NP / 8; ++nt) {
-                float d[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-                for (int ks = 0; ks < KP / 16; ++ks) {
-                    const __nv_bfloat16 *A0 = As + (a * kTile + r0 + gq) * KS + ks * 16 + 2 * tq;
-                    const __nv_bfloat16 *A1 = A0 + 8 * KS;
-                    const uint32_t a0 = *reinterpret_cast<const uint32_t *>(A0);
-                    const uint32_t a1 = *reinterpret_cast<const uint32_t *>(A1);
-                    const uint32_t a2 = *reinterpret_cast<const uint32_t *>(A0 + 8);
-                    const uint32_t a3 = *reinterpret_cast<const uint32_t *>(A1 + 8);
-                    const __nv_bfloat16 *B0 = Bs + (nt * 8 + gq) * KS + ks * 16 + 2 * tq;
-                    const uint32_t b0 = *reinterpret_cast<const uint32_t *>(B0);
-                    const uint32_t b1 = *reinterpret_cast<const uint32_t *>(B0 + 8);
-                    mma_bf16(d, a0, a1, a2, a3, b0, b1);
-                }
-                const int o = nt * 4 + tq;  // columns 2*tq, 2*tq+1 = (re, im) of channel o
-                if (o < COUT) {
-                    const int s0 = base + r0 + gq, s1 = s0 + 8;
-                    float2 *plane = out + (size_t)((o * 2 + par) * 3 + a) * pv;
-                    if (s0 < g.vh) plane[s0] = make_float2(d[0], d[1]);
-                    if (s1 < g.vh) plane[s1] = make_float2(d[2], d[3]);
-                }
+                for (int o = 0; o < COUT; ++o)
+                    out[(size_t)((o * 2 + par) * 3 + a) * pv + site] = make_float2(d[2 * o], d[2 * o + 1]);
             }
         }
     }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tbase, kTmemCols);
 }
 
 // ---------------------------------------------------------------------------------------------------- weight grad
@@ -183,7 +236,7 @@ __global__ void __launch_bounds__(kThr) ptc_wgrad_kernel(Geom g, int pv, LinkSet
                                                          int swap_paths)
 {
     constexpr int KP = kpad_of(CIN), NP = npad_of(COUT), RS = kTile + 8;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     __nv_bfloat16 *Tt = reinterpret_cast<__nv_bfloat16 *>(smem_raw);  // [3][KP][RS]
     __nv_bfloat16 *Gt = Tt + 3 * KP * RS;                             // [3][NP][RS]
     const int tiles_per_par = (g.vh + kTile - 1) / kTile;
@@ -194,8 +247,12 @@ __global__ void __launch_bounds__(kThr) ptc_wgrad_kernel(Geom g, int pv, LinkSet
     for (int a = 0; a < 3; ++a)
         for (int k = 0; k < KP; ++k) Tt[(a * KP + k) * RS + t] = __float2bfloat16_rn(0.f);
     if (i < g.vh) {
-        gather_site<CIN>(g, pv, fat, in, par, i, swap_paths != 0, [&](int a, int k, float v) {
-            Tt[(a * KP + k) * RS + t] = __float2bfloat16_rn(v);
+        gather_paths<CIN>(g, pv, fat, in, par, i, swap_paths != 0, [&](int p, const float (&vals)[3][2 * CIN]) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int j = 0; j < 2 * CIN; ++j)
+                    Tt[(a * KP + p * 2 * CIN + j) * RS + t] = __float2bfloat16_rn(vals[a][j]);
         });
     }
 #pragma unroll
@@ -325,9 +382,37 @@ __global__ void ptc_adam_kernel(float *w, const float *grad, float *m, float *v,
 
 // ---------------------------------------------------------------------------------------------------- host side
 template <int CIN, int COUT>
-static size_t fwd_smem() { return (size_t)(3 * kTile + npad_of(COUT)) * (kpad_of(CIN) + 8) * 2; }
+static size_t fwd_smem() { return (size_t)(3 * kTile + kNT) * kpad_of(CIN) * 2 + 16; }
 template <int CIN, int COUT>
 static size_t wgrad_smem() { return (size_t)3 * (kpad_of(CIN) + npad_of(COUT)) * (kTile + 8) * 2; }
+
+// device word the forward kernels set when a tile's tensor-core work did not complete in time
+__device__ int g_ptc_fault;
+
+static int *fault_flag()
+{
+    static int *ptr[64] = {nullptr};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return nullptr;
+    if (!ptr[dev] && cudaGetSymbolAddress(reinterpret_cast<void **>(&ptr[dev]), g_ptc_fault) != cudaSuccess)
+        ptr[dev] = nullptr;
+    return ptr[dev];
+}
+
+cudaError_t ptc_check_fault(cudaStream_t s)
+{
+    int *f = fault_flag();
+    if (!f) return cudaErrorInvalidDevicePointer;
+    int h = 0;
+    KQ_CUDA_TRY(cudaMemcpyAsync(&h, f, sizeof(int), cudaMemcpyDeviceToHost, s));
+    KQ_CUDA_TRY(cudaStreamSynchronize(s));
+    if (h) {
+        set_last_error("ptc: tensor-core tile did not complete within the wait limit");
+        return cudaErrorLaunchTimeout;
+    }
+    return cudaSuccess;
+}
 
 template <int CIN, int COUT>
 static cudaError_t run_forward(const Geom &g, const LinkSet &fat, const float2 *in, float2 *out,
@@ -338,7 +423,9 @@ static cudaError_t run_forward(const Geom &g, const LinkSet &fat, const float2 *
     const size_t sm = fwd_smem<CIN, COUT>();
     KQ_CUDA_TRY(cudaFuncSetAttribute(ptc_forward_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sm));
-    ptc_forward_kernel<CIN, COUT><<<tiles, kThr, sm, s>>>(g, pv, fat, in, out, Bt, swap ? 1 : 0);
+    int *fault = fault_flag();
+    if (!fault) return cudaErrorInvalidDevicePointer;
+    ptc_forward_kernel<CIN, COUT><<<tiles, kThr, sm, s>>>(g, pv, fat, in, out, Bt, swap ? 1 : 0, fault);
     return cudaGetLastError();
 }
 

@@ -5,7 +5,7 @@
 namespace kq {
 
 // One layer, cin -> cout channels (1 or 8), on full-lattice activations (layout in kq_ptc.cu).  Bt: [npad][kpad]
-// BF16 GEMM matrix built from the complex weights.  swap = true gathers the hops with swapped path labels (the
+// BF16 GEMM matrix built from the complex weights, column k = (p * cin + i) * 2 + reim for path p, input channel i.  swap = true gathers the hops with swapped path labels (the
 // adjoint layer, with conjugate-transposed weights).
 cudaError_t ptc_forward(const Geom &g, const LinkSet &fat, int cin, int cout, const float2 *in, float2 *out,
                         const void *Bt, bool swap, cudaStream_t s);
@@ -13,6 +13,9 @@ cudaError_t ptc_forward(const Geom &g, const LinkSet &fat, int cin, int cout, co
 // adjoint layer -- and G: the output gradient)
 cudaError_t ptc_wgrad(const Geom &g, const LinkSet &fat, int cin, int cout, const float2 *in, const float2 *gout,
                       float *partial, float *dB, bool swap, cudaStream_t s);
+// cudaErrorLaunchTimeout when a forward tile's tensor-core work did not complete within its wait limit (the
+// kernels then leave that tile unwritten); synchronises the stream
+cudaError_t ptc_check_fault(cudaStream_t s);
 int ptc_kpad(int cin);
 int ptc_npad(int cout);
 int ptc_tiles(const Geom &g);
