@@ -1,13 +1,16 @@
 """Stand-alone HISQ dslash driver: applies the even-odd dslash `--reps` times on synthetic fields and prints the
 achieved rate (1146 flop per output site; compulsory bytes 2400 / 1200 / 608 per site for DOUBLE / SINGLE /
-HALF).  Used for profiling the dslash kernels in isolation.
+HALF).  Used for profiling the dslash kernels in isolation.  With --ptc it applies the learned preconditioner
+M = N^dag N (N: 1 -> 8 -> 8 channels, random weights) instead, four tensor-core PTC layers per application.
 
     python -m kuqcd_b200.dslash_bench --dims 32 32 32 32 --prec double --reps 20
+    python -m kuqcd_b200.dslash_bench --dims 32 32 32 32 --ptc --reps 5
 """
 from __future__ import annotations
 
 import argparse
 import json
+import time
 
 import numpy as np
 import torch
@@ -25,6 +28,7 @@ def main():
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--eps", type=float, default=0.3)
+    ap.add_argument("--ptc", action="store_true", help="time the learned preconditioner's application instead")
     args = ap.parse_args()
     dims = tuple(args.dims)
     V = int(np.prod(dims))
@@ -39,6 +43,22 @@ def main():
     db = torch.empty(Vh * 6, dtype=torch.float64, device="cuda")
     ctx.make_source(1, 2, db)
     hb = db.cpu().numpy()
+    if args.ptc:
+        net = K.Net(ctx, (1, 8, 8))
+        net.weights = (0.3 * np.random.default_rng(0).standard_normal(net.nw)).astype(np.float32)
+        a = torch.zeros(ctx.spinor_bytes(K.KUQCD_DOUBLE), dtype=torch.uint8, device="cuda")
+        o = torch.zeros_like(a)
+        ctx.upload(K.KUQCD_DOUBLE, hb, a)
+        for _ in range(args.warmup):
+            net.apply(a, o, 1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.reps):
+            net.apply(a, o, 1)  # returns after its stream has drained
+        t = (time.perf_counter() - t0) / args.reps
+        print(json.dumps({"dims": list(dims), "ptc_apply_ms": t * 1e3, "layers": 4}))
+        net.close()
+        return
     stream = torch.cuda.Stream()
     out = {}
     for name in args.prec:
