@@ -91,6 +91,32 @@ KuQCDStatus kq_dslash_full(kq_context *ctx, int prec, const void *d_src, void *d
 KuQCDStatus kq_mdagm_full(kq_context *ctx, int prec, double sigma, const void *d_src, void *d_dst, void *d_tmp,
                           void *stream);
 
+/* ---------------------------------------------------------------- domain decomposition along t
+ * The multi-rank path of the reference's dslash (halo pack / exchange, dirac_hisq.cpp:236-407; Communicator,
+ * communication.cpp:73-138) for one GPU per rank.  Each rank's context holds its slab of the global lattice
+ * (local extents nx, ny, nz, nt_local; global t0 = rank * nt_local; nt_local even and >= 4).  The library packs
+ * faces into caller buffers; the caller moves them (NCCL send/recv, or any transport) and passes the received
+ * buffers to the dslash, which reads them in place:
+ *   ghost_lo of rank r = face_hi of rank r-1 (its top 3 t slices), ghost_hi of rank r = face_lo of rank r+1.
+ * Ghost links (t-direction links of the 3 slices below t0) are exchanged the same way once after loading:
+ * kq_slab_pack_link_face on rank r-1, kq_slab_set_link_ghosts on rank r. */
+KuQCDStatus kq_slab_set(kq_context *ctx, int rank, int nranks);
+size_t kq_slab_face_bytes(const kq_context *ctx, int prec);          /* one face: 3 t slices of one parity */
+KuQCDStatus kq_slab_pack_faces(kq_context *ctx, int prec, const void *d_src, void *d_face_lo, void *d_face_hi,
+                               void *stream);
+size_t kq_slab_link_face_bytes(const kq_context *ctx);               /* FP64 t links, 3 slices, both types */
+KuQCDStatus kq_slab_pack_link_face(kq_context *ctx, void *d_face);  /* top 3 slices, for rank + 1 */
+KuQCDStatus kq_slab_set_link_ghosts(kq_context *ctx, const void *d_face); /* received from rank - 1 */
+/* d_dst (parity dst_parity) = D d_src on the slab, or sigma * d_pvec - D d_src when d_pvec != NULL; DOUBLE or
+ * SINGLE.  Replaces DiracHISQ::Dslash with np > 1 (StartComm / interior / EndComm, dirac_hisq.cpp:409-455). */
+KuQCDStatus kq_slab_dslash(kq_context *ctx, int prec, const void *d_src, const void *d_ghost_lo,
+                           const void *d_ghost_hi, void *d_dst, int dst_parity, const void *d_pvec, double sigma,
+                           void *stream);
+/* BLAS-1 on FP64 fields of the context (spinor_field.cpp:130-252): y = a x + b y; local Re<x, y> (the caller
+ * sums it over ranks, as the reference's MPI_Allreduce does, spinor_field.cpp:207-215) */
+KuQCDStatus kq_field_axpby(kq_context *ctx, double a, const void *d_x, double b, void *d_y, void *stream);
+KuQCDStatus kq_field_dot(kq_context *ctx, const void *d_x, const void *d_y, double *out);
+
 /* ---------------------------------------------------------------- solver */
 enum {
     KQ_SOLVER_CGM = 0,        /* multishift CG with the reference's recurrences (CGM::Invert), FP64 or FP32 */

@@ -144,6 +144,8 @@ KQ_API void kq_context_destroy(kq_context *ctx)
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     for (int p = 0; p < 3; ++p) free_links(ctx, p);
+    for (void *gl : ctx->ghost_links)
+        if (gl) cudaFree(gl);
     if (ctx->work) cudaFree(ctx->work);
     if (ctx->d_scratch) cudaFree(ctx->d_scratch);
     if (ctx->poll) cudaFreeHost(ctx->poll);
@@ -192,6 +194,7 @@ KQ_API KuQCDStatus kq_load_links(kq_context *ctx, int link_type, const void *hos
     }
     if (link_type == KUQCD_FAT_LINK) ctx->fat_loaded = true;
     else ctx->long_loaded = true;
+    ctx->have_ghost[0] = ctx->have_ghost[1] = false;  // a slab's ghost links belong to the previous links
     ctx->gd.have[mp] = ctx->fat_loaded && ctx->long_loaded;
     // derived copies are stale now
     for (int p = 0; p < 3; ++p)

@@ -16,6 +16,12 @@ struct kq_context {
     void *work = nullptr;
     size_t work_bytes = 0;
     kq::CgmPoll *poll = nullptr;  // pinned host page for state polling
+    // t-slab of a domain-decomposed lattice (kq_slab.cu): this context holds local t = 0 .. nt-1 of global
+    // t0 = slab_rank * nt; ghost links are the t-direction fat and long links of the 3 slices below t0, per
+    // precision (P64, P32): [fat par0 | fat par1 | long par0 | long par1], each one direction of 3 slices
+    int slab_rank = -1, slab_nranks = 0;
+    void *ghost_links[2] = {nullptr, nullptr};
+    bool have_ghost[2] = {false, false};
 };
 
 namespace kq {

@@ -1,0 +1,386 @@
+// Domain decomposition along t: one context per rank holds the slab t0 = rank * nt_local .. t0 + nt_local - 1 of
+// the global lattice; the dslash's t hops that leave the slab read ghost slices received from the neighbouring
+// ranks.  This is the multi-rank path of the reference's dslash (halo pack / exchange / unpack,
+// dirac_hisq.cpp:236-407, and the Communicator of communication.cpp:73-138), restated for GPUs: the faces are
+// packed by a kernel into the sender's own buffer, the caller moves them (NCCL send/recv over NVLink, or any
+// transport), and the dslash reads the received buffers in place -- there is no unpack step.
+//
+// Geometry.  The local extent nt_local is even and >= 4, so local and global site parities agree and a depth-3
+// halo comes from one neighbour.  Every t slice of one parity holds S = nx*ny*nz/2 sites, contiguous in the
+// checkerboard index (i = j + S*t, j the index inside the slice), so a face of 3 slices is 3*S consecutive sites
+// of every plane.  Ghost fields use the device spinor layout with pitch pad(3*S): slot s of the lower ghost is
+// global t0 - 3 + s, slot s of the upper ghost is t0 + nt_local + s.
+//
+// Links.  Forward hops use the link at the output site (local).  Backward t hops from t < 3 need the t-direction
+// fat link of slice -1 and long links of slices -3..-1, owned by the rank below: that rank packs its top 3 slices
+// of t links (kq_slab_pack_link_face), the caller delivers them once after loading, and kq_slab_set_link_ghosts
+// stores them (FP64, with an FP32 copy made on first use).
+#include <algorithm>
+#include <vector>
+
+#include "kq_context.h"
+#include "kq_dslash_core.cuh"
+
+namespace kq {
+
+struct SlabArgs {
+    const void *glo, *ghi;  // ghost spinors (other parity), pitch pvg
+    int pvg;
+    const void *gfat_q, *glng_q;  // ghost t links of the other parity (one direction, 3 slices), pitch pvg
+    const void *pvec;             // optional: dst = sigma * pvec - D src
+    double sigma;
+};
+
+// D src at output site i (parity p) of the slab; same term order as dslash_site2, so results match the
+// undecomposed operator bit for bit.
+template <int P>
+__device__ __forceinline__ void slab_site(const Geom &g, int pv, const LinkSet &fat, const LinkSet &lng,
+                                          const void *src, const SlabArgs &a, int p, int i,
+                                          typename Acc2<P, P>::T acc[6])
+{
+    using T = typename Acc2<P, P>::T;
+    const SiteCoord c = site_coord(g, i, p);
+    const void *fat_p = p ? fat.par[1] : fat.par[0], *fat_q = p ? fat.par[0] : fat.par[1];
+    const void *lng_p = p ? lng.par[1] : lng.par[0], *lng_q = p ? lng.par[0] : lng.par[1];
+    const int S = g.st, lt = g.n[3];
+    const int j = i - c.t * S;  // index inside the t slice
+#pragma unroll
+    for (int k = 0; k < 6; ++k) acc[k] = T(0);
+#pragma unroll
+    for (int dir = 0; dir < 4; ++dir) {
+        T u[18], v[6];
+        if (dir < 3) {
+            const int nf1 = nbr_index(g, c, i, dir, 1);
+            const int nf3 = nbr_index(g, c, i, dir, 3);
+            const int nb1 = nbr_index(g, c, i, dir, -1);
+            const int nb3 = nbr_index(g, c, i, dir, -3);
+            ld_link<P>(fat_p, pv, dir, i, fat.scale, u);
+            ld_spinor<P>(src, pv, nf1, v);
+            mv_add(u, v, acc);
+            ld_link<P>(lng_p, pv, dir, i, lng.scale, u);
+            ld_spinor<P>(src, pv, nf3, v);
+            mv_add(u, v, acc);
+            ld_link<P>(fat_q, pv, dir, nb1, fat.scale, u);
+            ld_spinor<P>(src, pv, nb1, v);
+            mdv_sub(u, v, acc);
+            ld_link<P>(lng_q, pv, dir, nb3, lng.scale, u);
+            ld_spinor<P>(src, pv, nb3, v);
+            mdv_sub(u, v, acc);
+        } else {
+            // forward hops: upper ghost slot t + h - lt when the hop leaves the slab
+#pragma unroll
+            for (int h = 1; h <= 3; h += 2) {
+                const int tt = c.t + h;
+                ld_link<P>(h == 1 ? fat_p : lng_p, pv, 3, i, h == 1 ? fat.scale : lng.scale, u);
+                if (tt < lt) ld_spinor<P>(src, pv, i + h * S, v);
+                else ld_spinor<P>(a.ghi, a.pvg, (tt - lt) * S + j, v);
+                mv_add(u, v, acc);
+            }
+            // backward hops: lower ghost slot t - h + 3 (spinor and link) when the hop leaves the slab
+#pragma unroll
+            for (int h = 1; h <= 3; h += 2) {
+                const int tt = c.t - h;
+                if (tt >= 0) {
+                    ld_link<P>(h == 1 ? fat_q : lng_q, pv, 3, i - h * S, h == 1 ? fat.scale : lng.scale, u);
+                    ld_spinor<P>(src, pv, i - h * S, v);
+                } else {
+                    ld_link<P>(h == 1 ? a.gfat_q : a.glng_q, a.pvg, 0, (tt + 3) * S + j, 1.f, u);
+                    ld_spinor<P>(a.glo, a.pvg, (tt + 3) * S + j, v);
+                }
+                mdv_sub(u, v, acc);
+            }
+        }
+    }
+}
+
+template <int P>
+__global__ void __launch_bounds__(256) slab_dslash_kernel(Geom g, int pv, LinkSet fat, LinkSet lng,
+                                                          const void *__restrict__ src, SlabArgs a,
+                                                          void *__restrict__ dst, int p)
+{
+    using T = typename Acc2<P, P>::T;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.vh) return;
+    T acc[6];
+    slab_site<P>(g, pv, fat, lng, src, a, p, i, acc);
+    if (a.pvec) {
+        T pv6[6];
+        ld_spinor<P>(a.pvec, pv, i, pv6);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) acc[k] = (T)a.sigma * pv6[k] - acc[k];
+    }
+    st_spinor<P>(dst, pv, i, acc);
+}
+
+// faces of a spinor: lo = slices 0..2, hi = slices lt-3..lt-1 (pitch pvg)
+template <int P>
+__global__ void slab_pack_kernel(Geom g, int pv, const void *__restrict__ src, int pvg, void *__restrict__ lo,
+                                 void *__restrict__ hi)
+{
+    const int S = g.st, n = 3 * S;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    typename Acc<P>::T v[6];
+    ld_spinor<P>(src, pv, k, v);
+    st_spinor<P>(lo, pvg, k, v);
+    ld_spinor<P>(src, pv, (g.n[3] - 3) * S + k, v);
+    st_spinor<P>(hi, pvg, k, v);
+}
+
+// top 3 slices of the t-direction FP64 links (fat and long, both parities) -> face [fat p0|fat p1|lng p0|lng p1]
+__global__ void slab_link_pack_kernel(Geom g, int pv, LinkSet fat, LinkSet lng, int pvg, size_t part_bytes,
+                                      char *__restrict__ face)
+{
+    const int S = g.st, n = 3 * S;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = (g.n[3] - 3) * S + k;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const LinkSet &L = q < 2 ? fat : lng;
+        double u[18];
+        ld_link<0>(q & 1 ? L.par[1] : L.par[0], pv, 3, i, 1.f, u);
+        st_link<0>(face + q * part_bytes, pvg, 0, k, 1.f, u);
+    }
+}
+
+// FP64 ghost links -> FP32 copy
+__global__ void slab_link_to32_kernel(int n, int pvg, size_t part64, const char *__restrict__ g64, size_t part32,
+                                      char *__restrict__ g32)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        double u[18];
+        ld_link<0>(g64 + q * part64, pvg, 0, k, 1.f, u);
+        st_link<1>(g32 + q * part32, pvg, 0, k, 1.f, u);
+    }
+}
+
+// y = a x + b y on FP64 fields (pitch pv), and the block partials of <x, y>
+__global__ void field_axpby_kernel(int vh, int pv, double a, const void *__restrict__ x, double b, void *y)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= vh) return;
+    double xv[6], yv[6];
+    ld_spinor<0>(x, pv, i, xv);
+    ld_spinor<0>(y, pv, i, yv);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) yv[k] = a * xv[k] + b * yv[k];
+    st_spinor<0>(y, pv, i, yv);
+}
+
+__global__ void __launch_bounds__(256) field_dot_kernel(int vh, int pv, const void *__restrict__ x,
+                                                        const void *__restrict__ y, double *partials)
+{
+    __shared__ double sm[32];
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    double s = 0.0;
+    if (i < vh) {
+        double xv[6], yv[6];
+        ld_spinor<0>(x, pv, i, xv);
+        ld_spinor<0>(y, pv, i, yv);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) s += xv[k] * yv[k];
+    }
+    s = block_sum(s, sm);
+    if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+static int face_sites(const Geom &g) { return 3 * g.st; }
+static int face_pitch(const Geom &g) { return pad_sites(face_sites(g)); }
+
+static size_t ghost_link_part(const Geom &g, int prec)  // one type, one parity, one direction, 3 slices
+{
+    return (size_t)(prec == P64 ? 144 : 72) * face_pitch(g);
+}
+
+}  // namespace kq
+
+using namespace kq;
+
+#define KQ_API extern "C" __attribute__((visibility("default")))
+
+static KuQCDStatus slab_check(const kq_context *ctx, const char *where)
+{
+    if (!ctx) return KUQCD_ERR_NULL_POINTER;
+    if (ctx->slab_nranks < 1) {
+        set_last_error(std::string(where) + ": the context is not a slab (kq_slab_set)");
+        return KUQCD_ERR_UNEXPECTED_CALL_ORDER;
+    }
+    return KUQCD_SUCCESS;
+}
+
+KQ_API KuQCDStatus kq_slab_set(kq_context *ctx, int rank, int nranks)
+{
+    if (!ctx) return KUQCD_ERR_NULL_POINTER;
+    const int lt = ctx->g.n[3];
+    if (nranks < 1 || rank < 0 || rank >= nranks || lt < 4 || (lt & 1)) {
+        set_last_error("kq_slab_set: 0 <= rank < nranks, and the local t extent must be even and >= 4");
+        return KUQCD_ERR_INVALID_PARAM;
+    }
+    ctx->slab_rank = rank;
+    ctx->slab_nranks = nranks;
+    ctx->have_ghost[0] = ctx->have_ghost[1] = false;
+    return KUQCD_SUCCESS;
+}
+
+KQ_API size_t kq_slab_face_bytes(const kq_context *ctx, int prec)
+{
+    const int p = ctx ? prec_from_api(prec) : -1;
+    if (p < 0) return 0;
+    const size_t per_site = p == P64 ? 48 : p == P32 ? 24 : 16;
+    return per_site * face_pitch(ctx->g);
+}
+
+KQ_API KuQCDStatus kq_slab_pack_faces(kq_context *ctx, int prec, const void *d_src, void *d_face_lo, void *d_face_hi,
+                                      void *stream)
+{
+    KuQCDStatus st = slab_check(ctx, "kq_slab_pack_faces");
+    if (st != KUQCD_SUCCESS) return st;
+    if (!d_src || !d_face_lo || !d_face_hi) return KUQCD_ERR_NULL_POINTER;
+    const int p = prec_from_api(prec);
+    if (p < 0) return KUQCD_ERR_INVALID_PARAM;
+    cudaSetDevice(ctx->device);
+    const Geom &g = ctx->g;
+    const int n = face_sites(g), pv = pad_sites(g.vh), pvg = face_pitch(g);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    const int nb = (n + 255) / 256;
+    if (p == P64) slab_pack_kernel<0><<<nb, 256, 0, s>>>(g, pv, d_src, pvg, d_face_lo, d_face_hi);
+    else if (p == P32) slab_pack_kernel<1><<<nb, 256, 0, s>>>(g, pv, d_src, pvg, d_face_lo, d_face_hi);
+    else slab_pack_kernel<2><<<nb, 256, 0, s>>>(g, pv, d_src, pvg, d_face_lo, d_face_hi);
+    return status_of(cudaGetLastError());
+}
+
+KQ_API size_t kq_slab_link_face_bytes(const kq_context *ctx)
+{
+    return ctx ? 4 * ghost_link_part(ctx->g, P64) : 0;
+}
+
+KQ_API KuQCDStatus kq_slab_pack_link_face(kq_context *ctx, void *d_face)
+{
+    KuQCDStatus st = slab_check(ctx, "kq_slab_pack_link_face");
+    if (st != KUQCD_SUCCESS) return st;
+    if (!d_face) return KUQCD_ERR_NULL_POINTER;
+    if (!ctx->gd.have[P64]) {
+        st = kq_prepare_links(ctx, KUQCD_DOUBLE);
+        if (st != KUQCD_SUCCESS) return st;
+    }
+    cudaSetDevice(ctx->device);
+    const Geom &g = ctx->g;
+    const int n = face_sites(g);
+    slab_link_pack_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(g, pad_sites(g.vh), ctx->gd.fat[P64],
+                                                                     ctx->gd.lng[P64], face_pitch(g),
+                                                                     ghost_link_part(g, P64),
+                                                                     static_cast<char *>(d_face));
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    return status_of(e);
+}
+
+KQ_API KuQCDStatus kq_slab_set_link_ghosts(kq_context *ctx, const void *d_face)
+{
+    KuQCDStatus st = slab_check(ctx, "kq_slab_set_link_ghosts");
+    if (st != KUQCD_SUCCESS) return st;
+    if (!d_face) return KUQCD_ERR_NULL_POINTER;
+    cudaSetDevice(ctx->device);
+    const size_t bytes = 4 * ghost_link_part(ctx->g, P64);
+    cudaError_t e = cudaSuccess;
+    if (!ctx->ghost_links[0]) e = cudaMalloc(&ctx->ghost_links[0], bytes);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->ghost_links[0], d_face, bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    ctx->have_ghost[0] = e == cudaSuccess;
+    ctx->have_ghost[1] = false;
+    return status_of(e);
+}
+
+static cudaError_t ensure_ghost32(kq_context *ctx)
+{
+    if (ctx->have_ghost[1]) return cudaSuccess;
+    const Geom &g = ctx->g;
+    if (!ctx->ghost_links[1]) KQ_CUDA_TRY(cudaMalloc(&ctx->ghost_links[1], 4 * ghost_link_part(g, P32)));
+    const int n = face_sites(g);
+    slab_link_to32_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(
+        n, face_pitch(g), ghost_link_part(g, P64), static_cast<const char *>(ctx->ghost_links[0]),
+        ghost_link_part(g, P32), static_cast<char *>(ctx->ghost_links[1]));
+    KQ_CUDA_TRY(cudaGetLastError());
+    ctx->have_ghost[1] = true;
+    return cudaSuccess;
+}
+
+KQ_API KuQCDStatus kq_slab_dslash(kq_context *ctx, int prec, const void *d_src, const void *d_ghost_lo,
+                                  const void *d_ghost_hi, void *d_dst, int dst_parity, const void *d_pvec,
+                                  double sigma, void *stream)
+{
+    KuQCDStatus st = slab_check(ctx, "kq_slab_dslash");
+    if (st != KUQCD_SUCCESS) return st;
+    if (!d_src || !d_ghost_lo || !d_ghost_hi || !d_dst) return KUQCD_ERR_NULL_POINTER;
+    const int p = prec_from_api(prec);
+    if ((p != P64 && p != P32) || (dst_parity != 0 && dst_parity != 1)) {
+        set_last_error("kq_slab_dslash: DOUBLE or SINGLE, parity 0 or 1");
+        return KUQCD_ERR_INVALID_PARAM;
+    }
+    if (!ctx->have_ghost[0]) {
+        set_last_error("kq_slab_dslash: ghost links not set (kq_slab_set_link_ghosts)");
+        return KUQCD_ERR_UNEXPECTED_CALL_ORDER;
+    }
+    if (!ctx->gd.have[p]) {
+        st = kq_prepare_links(ctx, prec);
+        if (st != KUQCD_SUCCESS) return st;
+    }
+    cudaSetDevice(ctx->device);
+    cudaError_t e = p == P32 ? ensure_ghost32(ctx) : cudaSuccess;
+    if (e != cudaSuccess) return status_of(e);
+    const Geom &g = ctx->g;
+    const size_t part = ghost_link_part(g, p);
+    const char *gl = static_cast<const char *>(ctx->ghost_links[p]);
+    const int q = 1 - dst_parity;
+    SlabArgs a;
+    a.glo = d_ghost_lo;
+    a.ghi = d_ghost_hi;
+    a.pvg = face_pitch(g);
+    a.gfat_q = gl + (0 + q) * part;
+    a.glng_q = gl + (2 + q) * part;
+    a.pvec = d_pvec;
+    a.sigma = sigma;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    const int nb = (g.vh + 255) / 256, pv = pad_sites(g.vh);
+    if (p == P64)
+        slab_dslash_kernel<0><<<nb, 256, 0, s>>>(g, pv, ctx->gd.fat[P64], ctx->gd.lng[P64], d_src, a, d_dst, dst_parity);
+    else
+        slab_dslash_kernel<1><<<nb, 256, 0, s>>>(g, pv, ctx->gd.fat[P32], ctx->gd.lng[P32], d_src, a, d_dst, dst_parity);
+    return status_of(cudaGetLastError());
+}
+
+KQ_API KuQCDStatus kq_field_axpby(kq_context *ctx, double a, const void *d_x, double b, void *d_y, void *stream)
+{
+    if (!ctx || !d_x || !d_y) return KUQCD_ERR_NULL_POINTER;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    const Geom &g = ctx->g;
+    field_axpby_kernel<<<(g.vh + 255) / 256, 256, 0, s>>>(g.vh, pad_sites(g.vh), a, d_x, b, d_y);
+    return status_of(cudaGetLastError());
+}
+
+KQ_API KuQCDStatus kq_field_dot(kq_context *ctx, const void *d_x, const void *d_y, double *out)
+{
+    if (!ctx || !d_x || !d_y || !out) return KUQCD_ERR_NULL_POINTER;
+    cudaSetDevice(ctx->device);
+    const Geom &g = ctx->g;
+    const int nb = (g.vh + 255) / 256;
+    Carve probe(nullptr);
+    probe.take(sizeof(double) * nb);
+    cudaError_t e = ensure_work(ctx, probe.off);
+    if (e != cudaSuccess) return status_of(e);
+    double *partials = static_cast<double *>(ctx->work);
+    field_dot_kernel<<<nb, 256, 0, ctx->stream>>>(g.vh, pad_sites(g.vh), d_x, d_y, partials);
+    std::vector<double> h(nb);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), partials, sizeof(double) * nb, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    double sum = 0;
+    for (double v : h) sum += v;
+    *out = sum;
+    return status_of(e);
+}

@@ -63,7 +63,9 @@ EXPORTED_SYMBOLS = [
     "kq_kuqcd_init", "kq_kuqcd_load_gaugefield", "kq_kuqcd_solve_multishift", "kq_kuqcd_gauge_free",
     "kq_kuqcd_end", "kq_context_create", "kq_context_destroy", "kq_load_links", "kq_prepare_links",
     "kq_spinor_bytes", "kq_spinor_upload", "kq_spinor_download", "kq_spinor_convert", "kq_dslash", "kq_mdagm",
-    "kq_mdagm_noalloc", "kq_dslash_full", "kq_mdagm_full",
+    "kq_mdagm_noalloc", "kq_dslash_full", "kq_mdagm_full", "kq_slab_set", "kq_slab_face_bytes",
+    "kq_slab_pack_faces", "kq_slab_link_face_bytes", "kq_slab_pack_link_face", "kq_slab_set_link_ghosts",
+    "kq_slab_dslash", "kq_field_axpby", "kq_field_dot",
     "kq_solve_multishift", "kq_solve_multishift_device", "kq_true_residuals", "kq_make_links_record",
     "kq_make_source_record", "kq_last_error", "kq_batch_create", "kq_batch_destroy", "kq_batch_add",
     "kq_batch_size", "kq_batch_solve", "kq_batch_system_info", "kq_net_create", "kq_net_destroy",
@@ -117,6 +119,15 @@ def library() -> C.CDLL:
         "kq_mdagm_noalloc": (i, [vp, i, d, vp, vp, i, vp]),
         "kq_dslash_full": (i, [vp, i, vp, vp, vp]),
         "kq_mdagm_full": (i, [vp, i, d, vp, vp, vp, vp]),
+        "kq_slab_set": (i, [vp, i, i]),
+        "kq_slab_face_bytes": (sz, [vp, i]),
+        "kq_slab_pack_faces": (i, [vp, i, vp, vp, vp, vp]),
+        "kq_slab_link_face_bytes": (sz, [vp]),
+        "kq_slab_pack_link_face": (i, [vp, vp]),
+        "kq_slab_set_link_ghosts": (i, [vp, vp]),
+        "kq_slab_dslash": (i, [vp, i, vp, vp, vp, vp, i, vp, d, vp]),
+        "kq_field_axpby": (i, [vp, d, vp, d, vp, vp]),
+        "kq_field_dot": (i, [vp, vp, vp, C.POINTER(d)]),
         "kq_solve_multishift": (i, [vp, C.POINTER(SolveParam), vp, C.POINTER(vp), C.POINTER(SolveInfo)]),
         "kq_solve_multishift_device": (i, [vp, C.POINTER(SolveParam), vp, vp, C.POINTER(SolveInfo)]),
         "kq_true_residuals": (i, [vp, i, i, C.POINTER(d), vp, vp, C.POINTER(d)]),

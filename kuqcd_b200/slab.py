@@ -1,0 +1,248 @@
+"""Domain decomposition along t: one slab of the global lattice per rank (one GPU per rank), halo exchange through
+a transport, and the reference's multishift CG (inverter_cgm.cpp:17-87) over the slabs with its reductions summed
+across ranks (spinor_field.cpp:207-215, 235-243).
+
+The kernels are in libkuqcd_b200.so (kq_slab.cu): face packing into the sender's buffers and a dslash that reads
+the received ghost buffers in place.  Transports move the faces:
+
+    TorchTransport   one rank per process over torch.distributed: NCCL for device buffers (NVLink), gloo for host
+                     buffers.  Two phases per exchange (faces going up in t, then down), so that with two ranks the
+                     point-to-point messages between the same pair are matched in order.
+    LocalTransport   every rank in this process: the ghost of a rank IS its neighbour's face buffer (no copy).
+                     Used to run a decomposed solve on one GPU, where ranks cannot run concurrently.
+
+Code written against a list of local slabs runs unchanged under both (SPMD over `slabs`).
+
+    slabs = [Slab(global_dims, r, R) for r in range(R)]              # or [Slab(global_dims, rank, world)]
+    for s in slabs: s.load_links(slab_of_links(fat, global_dims, s.rank, R), slab_of_links(lng, ...))
+    exchange_link_ghosts(slabs, transport)
+    xs, iters = cgm(slabs, transport, [b_r ...], shifts_ref, tol, max_iter)
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import lib as L
+
+
+def _p(t):
+    return L._ptr(t)
+
+
+# ---------------------------------------------------------------------------------------------------- host slicing
+def slab_of_links(record: np.ndarray, global_dims, rank: int, nranks: int) -> np.ndarray:
+    """Local NORMAL_ORDER link record (even sites then odd sites, 72 values per site) of one rank's slab."""
+    nx, ny, nz, nt = global_dims
+    lt, S = nt // nranks, nx * ny * nz // 2
+    vh = nx * ny * nz * nt // 2
+    rec = record.reshape(2, vh, 72)
+    return np.ascontiguousarray(rec[:, rank * lt * S:(rank + 1) * lt * S]).reshape(-1)
+
+
+def slab_of_spinor(record: np.ndarray, global_dims, rank: int, nranks: int) -> np.ndarray:
+    """Local record (Vh_local * 6 values) of one parity field."""
+    nx, ny, nz, nt = global_dims
+    lt, S = nt // nranks, nx * ny * nz // 2
+    return np.ascontiguousarray(record.reshape(-1, 6)[rank * lt * S:(rank + 1) * lt * S]).reshape(-1)
+
+
+def join_spinor(parts) -> np.ndarray:
+    """Inverse of slab_of_spinor over all ranks (t is the slowest index of the checkerboard order)."""
+    return np.concatenate([np.asarray(p).reshape(-1) for p in parts])
+
+
+# ---------------------------------------------------------------------------------------------------- transports
+class LocalTransport:
+    """All ranks in this process: ghosts are the neighbours' face buffers; reductions are plain sums."""
+
+    def exchange(self, faces):
+        R = len(faces)
+        return [(faces[(r - 1) % R][1], faces[(r + 1) % R][0]) for r in range(R)]
+
+    def allreduce(self, values):
+        tot = np.sum(np.asarray(values, dtype=np.float64), axis=0)
+        return [tot.copy() for _ in values]
+
+
+class TorchTransport:
+    """One rank per process over torch.distributed (the process group must exist)."""
+
+    def __init__(self, group=None):
+        import torch.distributed as dist
+
+        self.dist = dist
+        self.group = group
+        self.rank = dist.get_rank(group)
+        self.world = dist.get_world_size(group)
+
+    def _peer(self, d):
+        r = (self.rank + d) % self.world
+        return self.dist.get_global_rank(self.group, r) if self.group is not None else r
+
+    def exchange(self, faces):
+        (lo, hi), = faces
+        if self.world == 1:
+            return [(hi, lo)]
+        d = self.dist
+        ghost_lo, ghost_hi = torch.empty_like(hi), torch.empty_like(lo)
+        # up in t: my top face becomes the lower ghost of rank + 1
+        ops = [d.P2POp(d.isend, hi, self._peer(1), self.group), d.P2POp(d.irecv, ghost_lo, self._peer(-1), self.group)]
+        for w in d.batch_isend_irecv(ops):
+            w.wait()
+        # down in t: my bottom face becomes the upper ghost of rank - 1
+        ops = [d.P2POp(d.isend, lo, self._peer(-1), self.group), d.P2POp(d.irecv, ghost_hi, self._peer(1), self.group)]
+        for w in d.batch_isend_irecv(ops):
+            w.wait()
+        if ghost_lo.is_cuda:
+            # NCCL completion orders only torch's current stream: the slab kernels run on the context's stream
+            torch.cuda.synchronize()
+        return [(ghost_lo, ghost_hi)]
+
+    def allreduce(self, values):
+        (v,) = values
+        dev = "cuda" if self.dist.get_backend(self.group) == "nccl" else "cpu"
+        t = torch.tensor(np.asarray(v, dtype=np.float64), device=dev)
+        self.dist.all_reduce(t, group=self.group)
+        return [t.cpu().numpy()]
+
+
+# ---------------------------------------------------------------------------------------------------- one slab
+class Slab:
+    """One rank's slab: a context of the local lattice (nx, ny, nz, nt / nranks) marked as slab `rank`."""
+
+    def __init__(self, global_dims, rank: int, nranks: int, device: int = 0):
+        nx, ny, nz, nt = global_dims
+        if nt % nranks:
+            raise ValueError("nt must be a multiple of the number of ranks")
+        self.global_dims = tuple(global_dims)
+        self.rank, self.nranks = rank, nranks
+        self.dims = (nx, ny, nz, nt // nranks)
+        self.device = device
+        self.ctx = L.Context(self.dims, device)
+        self.ctx._chk(L.library().kq_slab_set(self.ctx._h, rank, nranks), "kq_slab_set")
+        self._faces = {}
+
+    def field(self, prec=L.KUQCD_DOUBLE):
+        return torch.zeros(self.ctx.spinor_bytes(prec), dtype=torch.uint8, device=f"cuda:{self.device}")
+
+    def load_links(self, fat_local, lng_local):
+        self.ctx.load_links(L.KUQCD_FAT_LINK, fat_local)
+        self.ctx.load_links(L.KUQCD_LONG_LINK, lng_local)
+
+    def link_face(self):
+        n = L.library().kq_slab_link_face_bytes(self.ctx._h)
+        f = torch.empty(n, dtype=torch.uint8, device=f"cuda:{self.device}")
+        self.ctx._chk(L.library().kq_slab_pack_link_face(self.ctx._h, _p(f)), "kq_slab_pack_link_face")
+        return f
+
+    def set_link_ghosts(self, face):
+        self.ctx._chk(L.library().kq_slab_set_link_ghosts(self.ctx._h, _p(face)), "kq_slab_set_link_ghosts")
+
+    def pack(self, prec, src):
+        """(face_lo, face_hi) of src; the buffers are reused by the next pack of the same precision."""
+        if prec not in self._faces:
+            n = L.library().kq_slab_face_bytes(self.ctx._h, prec)
+            self._faces[prec] = tuple(torch.empty(n, dtype=torch.uint8, device=f"cuda:{self.device}")
+                                      for _ in range(2))
+        lo, hi = self._faces[prec]
+        self.ctx._chk(L.library().kq_slab_pack_faces(self.ctx._h, prec, _p(src), _p(lo), _p(hi), None),
+                      "kq_slab_pack_faces")
+        return lo, hi
+
+    def dslash(self, prec, src, ghost_lo, ghost_hi, dst, dst_parity, pvec=None, sigma=0.0):
+        self.ctx._chk(L.library().kq_slab_dslash(self.ctx._h, prec, _p(src), _p(ghost_lo), _p(ghost_hi), _p(dst),
+                                                 dst_parity, _p(pvec), float(sigma), None), "kq_slab_dslash")
+
+    def axpby(self, a, x, b, y):
+        self.ctx._chk(L.library().kq_field_axpby(self.ctx._h, float(a), _p(x), float(b), _p(y), None),
+                      "kq_field_axpby")
+
+    def dot(self, x, y) -> float:
+        out = C.c_double()
+        self.ctx._chk(L.library().kq_field_dot(self.ctx._h, _p(x), _p(y), C.byref(out)), "kq_field_dot")
+        return out.value
+
+    def close(self):
+        self.ctx.close()
+
+
+def exchange_link_ghosts(slabs, transport):
+    """Every rank gets the t links of the 3 slices below its slab from the rank below (once, after loading)."""
+    faces = [s.link_face() for s in slabs]
+    torch.cuda.synchronize()
+    # a link face travels up in t only: send it as the 'hi' face, receive it as the lower ghost
+    ghosts = transport.exchange([(f, f) for f in faces])
+    for s, (glo, _) in zip(slabs, ghosts):
+        s.set_link_ghosts(glo)
+
+
+def dslash(slabs, transport, prec, srcs, dsts, dst_parity, pvecs=None, sigma=0.0):
+    """dst_r = D src_r on every local slab (one halo exchange), or sigma * pvec_r - D src_r."""
+    faces = [s.pack(prec, x) for s, x in zip(slabs, srcs)]
+    torch.cuda.synchronize()
+    ghosts = transport.exchange(faces)
+    for k, (s, x, y, (glo, ghi)) in enumerate(zip(slabs, srcs, dsts, ghosts)):
+        s.dslash(prec, x, glo, ghi, y, dst_parity, None if pvecs is None else pvecs[k], sigma)
+    torch.cuda.synchronize()
+
+
+def cgm(slabs, transport, bs, shifts_ref, tol, max_iter, parity=0):
+    """Multishift CG of inverter_cgm.cpp:17-87 on FP64 slab fields.  shifts_ref: reference semantics (x_0 solves
+    shifts[0] - DD, x_j solves shifts[0] + shifts[j] - DD); stops shift k when Z_k^2 |r|^2 < tol.  Returns
+    (xs, iterations) with xs[r][k] the local solution of shift k on slab r."""
+    ns = len(shifts_ref)
+    D = L.KUQCD_DOUBLE
+
+    def allsum(vals):
+        return transport.allreduce([np.atleast_1d(np.asarray(v, dtype=np.float64)) for v in vals])[0]
+
+    r = [s.field() for s in slabs]
+    sv = [s.field() for s in slabs]
+    tmp = [s.field() for s in slabs]
+    p = [[s.field() for _ in range(ns)] for s in slabs]
+    x = [[s.field() for _ in range(ns)] for s in slabs]
+    for k, s in enumerate(slabs):
+        s.axpby(1.0, bs[k], 0.0, r[k])
+        for j in range(ns):
+            s.axpby(1.0, bs[k], 0.0, p[k][j])
+    a = np.zeros(ns)
+    B = np.ones(ns)
+    Z = np.ones(ns)
+    Zm1 = np.ones(ns)
+    rr = float(allsum([s.dot(rk, rk) for s, rk in zip(slabs, r)])[0])
+    Bm1, max_term, it = 1.0, ns, 0
+    while True:
+        it += 1
+        # s = shifts[0] p0 - D_pq D_qp p0 (MdaggM + Axmy, inverter_cgm.cpp:44-46)
+        dslash(slabs, transport, D, [pk[0] for pk in p], tmp, 1 - parity)
+        dslash(slabs, transport, D, tmp, sv, parity, pvecs=[pk[0] for pk in p], sigma=shifts_ref[0])
+        pAp = float(allsum([s.dot(pk[0], sk) for s, pk, sk in zip(slabs, p, sv)])[0])
+        B[0] = -rr / pAp
+        for k, s in enumerate(slabs):
+            s.axpby(B[0], sv[k], 1.0, r[k])
+        for j in range(1, max_term):
+            rr1 = Bm1 * Zm1[j] / (B[0] * a[0] * (Zm1[j] - Z[j]) + Zm1[j] * Bm1 * (1.0 - shifts_ref[j] * B[0]))
+            Zm1[j] = Z[j]
+            Z[j] = Z[j] * rr1
+            B[j] = B[0] * rr1
+        Bm1 = B[0]
+        lam2 = float(allsum([s.dot(rk, rk) for s, rk in zip(slabs, r)])[0])
+        a[0] = lam2 / rr
+        rr = lam2
+        for k, s in enumerate(slabs):
+            for j in range(max_term):
+                s.axpby(-B[j], p[k][j], 1.0, x[k][j])
+        for j in range(1, max_term):
+            a[j] = a[0] * Z[j] * B[j] / (Zm1[j] * B[0])
+        for k, s in enumerate(slabs):
+            for j in range(max_term):
+                s.axpby(Z[j], r[k], a[j], p[k][j])
+        while max_term > 0 and Z[max_term - 1] ** 2 * lam2 < tol:
+            max_term -= 1
+        if max_term == 0 or it >= max_iter:
+            break
+    torch.cuda.synchronize()
+    return x, it
