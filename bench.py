@@ -36,9 +36,13 @@ METRIC = "HISQ dslash GFLOP/s + HBM GB/s; multishift CG time to 1e-10, mixed vs 
 REL_RES = 1e-10
 DSLASH_FLOPS = 1146          # per output site
 DSLASH_BYTES = {8: 2400, 4: 1200, 2: 608}   # compulsory bytes per output site: 16 links + 1 in + 1 out spinor
+# Bytes an FP64 dslash moves per output site in its storage: with the long links compressed (two rows + 1/s,
+# 104 B) 8 x 144 + 8 x 104 + 96 = 2080; with full storage the compulsory 2400.
+DSLASH_FP64_STORAGE_BYTES = {1: 2080, 0: 2400}
 # DRAM traffic of one FP64 dslash_kernel launch per output site, from ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum = 1.238 GB at 32^4, Vh = 524,288: profiles/dslash_fp64_32x32x32x32.txt), scaled by sites
-DSLASH_FP64_TRAFFIC_PER_SITE = 1.238e9 / 524288
+# dram__bytes_write.sum at 32^4, Vh = 524,288: 1.073 GB compressed, profiles/dslash_fp64_recon_32x32x32x32.txt;
+# 1.238 GB full storage, profiles/dslash_fp64_32x32x32x32.txt), scaled by sites
+DSLASH_FP64_TRAFFIC_PER_SITE = {1: 1.073e9 / 524288, 0: 1.238e9 / 524288}
 # Workloads.  "32": 32^4, eps 0.3, m 0.05, 12 shifts 1e-4..1 (the default).  "48": 48^3x96, eps 0.4, m 0.02,
 # 16 shifts 1e-5..1.  ref_iters: iterations the reference CGM (inverter_cgm.cpp:17-87) needs on the workload
 # (seed 1000, tol (1e-10)^2 |b|^2, reference-semantics shifts): for 32^4 counted by running oracle/ref_iterations.py
@@ -214,6 +218,7 @@ def run_ours(args):
     dsl = {}
     # a dedicated (non-default) torch stream: the kernels run where the events are recorded
     stream = torch.cuda.Stream()
+    long_recon = ctx.long_links_compressed(K.KUQCD_DOUBLE)
     for name, prec in [("fp64", K.KUQCD_DOUBLE), ("fp32", K.KUQCD_SINGLE), ("half", K.KUQCD_HALF)]:
         nbp = ctx.spinor_bytes(prec)
         a = torch.zeros(nbp, dtype=torch.uint8, device="cuda")
@@ -280,7 +285,8 @@ def run_ours(args):
     peak = peaks.get("hbm_gbs")
     peak_note = "measured" if peak else "fallback"
     peak = peak or 6650.0
-    achieved = dsl[dom]["gbs"]
+    achieved = dsl[dom]["gbs"]  # SURVEY's compulsory 2400 B per site (18 reals per link)
+    storage_gbs = DSLASH_FP64_STORAGE_BYTES[long_recon] * Vh / (dsl[dom]["ms"] * 1e-3) / 1e9
 
     result = None
     if rank == 0:
@@ -320,10 +326,13 @@ def run_ours(args):
                     "d2h_bytes_per_step": NSHIFT * Vh * 6 * 8},
             "roofline": {"bound": "hbm", "kernel": f"dslash_kernel<{dom}>", "achieved": achieved, "peak": peak,
                          "peak_source": peak_note, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": DSLASH_FP64_TRAFFIC_PER_SITE * Vh,
+                         "traffic": DSLASH_FP64_TRAFFIC_PER_SITE[long_recon] * Vh,
                          "traffic_source": "ncu DRAM bytes of one launch at 32^4, scaled by output sites",
                          "algorithmic_bytes": DSLASH_BYTES[8] * Vh,
-                         "bytes_per_site": DSLASH_BYTES[8 if dom == 'fp64' else 4]},
+                         "bytes_per_site": DSLASH_BYTES[8 if dom == 'fp64' else 4],
+                         "long_links_compressed": bool(long_recon),
+                         "storage_bytes_per_site": DSLASH_FP64_STORAGE_BYTES[long_recon],
+                         "storage_gbs": storage_gbs, "storage_frac": storage_gbs / peak},
             "dslash": dsl,
             "cpu_baseline": cpu,
             "gpu_launches": launches,

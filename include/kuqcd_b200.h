@@ -54,6 +54,10 @@ KuQCDStatus kq_load_links(kq_context *ctx, int link_type, const void *host, int 
 /* Make both link fields resident in precision prec (SINGLE or HALF copies derived from the loaded master). */
 KuQCDStatus kq_prepare_links(kq_context *ctx, int prec);
 
+/* 1 when the long links of precision prec are stored compressed (two rows + 1/s; they are real multiples of SU(3)
+ * matrices, as HISQ's Naik links are), 0 for full storage, -1 when not resident.  Set KUQCD_LONG_RECON=0 to keep
+ * full storage.  (The reference's reconstruct options are stubs, su3.cpp:250-254; this one needs no caller input.) */
+KuQCDStatus kq_long_links_compressed(const kq_context *ctx, int prec, int *out);
 /* Bytes of one parity spinor field in the device layout of precision prec. */
 size_t kq_spinor_bytes(const kq_context *ctx, int prec);
 /* Host record (precision host_prec) <-> device field (precision prec).  Replaces kuqcd_spinorfield_set/get_values

@@ -153,6 +153,28 @@ KQ_API void kq_context_destroy(kq_context *ctx)
     delete ctx;
 }
 
+// Long links that are real multiples of SU(3) matrices (HISQ's Naik links: products of reunitarised links) are kept
+// as two rows + 1/s (104 B instead of 144 B per FP64 link, 52 B instead of 72 B in FP32): 13 % less traffic for
+// every FP64 and FP32 dslash.  KUQCD_LONG_RECON=0 keeps full storage.
+static cudaError_t compress_long(kq_context *ctx, int prec)
+{
+    const char *env = getenv("KUQCD_LONG_RECON");
+    if (env && env[0] == '0') return cudaSuccess;
+    if (prec != P64 && prec != P32) return cudaSuccess;
+    bool done = false;
+    return links_compress(ctx->g, ctx->gd.lng[prec], prec, prec == P64 ? 1e-12 : 2e-6, ctx->d_scratch, ctx->stream,
+                          &done);
+}
+
+KQ_API KuQCDStatus kq_long_links_compressed(const kq_context *ctx, int prec, int *out)
+{
+    if (!ctx || !out) return KUQCD_ERR_NULL_POINTER;
+    const int p = prec_from_api(prec);
+    if (p < 0) return KUQCD_ERR_INVALID_PARAM;
+    *out = ctx->gd.have[p] ? ctx->gd.lng[p].recon : -1;
+    return KUQCD_SUCCESS;
+}
+
 KQ_API KuQCDStatus kq_load_links(kq_context *ctx, int link_type, const void *host, int host_prec)
 {
     if (!ctx || !host) {
@@ -195,6 +217,13 @@ KQ_API KuQCDStatus kq_load_links(kq_context *ctx, int link_type, const void *hos
     if (link_type == KUQCD_FAT_LINK) ctx->fat_loaded = true;
     else ctx->long_loaded = true;
     ctx->have_ghost[0] = ctx->have_ghost[1] = false;  // a slab's ghost links belong to the previous links
+    if (link_type == KUQCD_LONG_LINK) {
+        e = compress_long(ctx, mp);
+        if (e != cudaSuccess) {
+            set_last_error(std::string("kq_load_links: ") + cudaGetErrorString(e));
+            return status_of(e);
+        }
+    }
     ctx->gd.have[mp] = ctx->fat_loaded && ctx->long_loaded;
     // derived copies are stale now
     for (int p = 0; p < 3; ++p)
@@ -222,6 +251,7 @@ KQ_API KuQCDStatus kq_prepare_links(kq_context *ctx, int prec)
     if (e == cudaSuccess)
         e = links_convert(ctx->g, ctx->gd.lng[ctx->master], ctx->master, ctx->gd.lng[p], p, ctx->d_scratch, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) e = compress_long(ctx, p);
     if (e != cudaSuccess) {
         free_links(ctx, p);
         set_last_error(std::string("kq_prepare_links: ") + cudaGetErrorString(e));

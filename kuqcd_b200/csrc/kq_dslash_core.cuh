@@ -113,13 +113,13 @@ __device__ __forceinline__ void dslash_site2(const Geom &g, int pv, const LinkSe
         ld_link<LP>(fat_p, pv, dir, i, fat.scale, u);
         ld_spinor<SP>(src, pv, nf1, v);
         mv_add(u, v, acc);
-        ld_link<LP>(lng_p, pv, dir, i, lng.scale, u);
+        ld_link_any<LP>(lng_p, pv, dir, i, lng.scale, lng.recon, u);
         ld_spinor<SP>(src, pv, nf3, v);
         mv_add(u, v, acc);
         ld_link<LP>(fat_q, pv, dir, nb1, fat.scale, u);
         ld_spinor<SP>(src, pv, nb1, v);
         mdv_sub(u, v, acc);
-        ld_link<LP>(lng_q, pv, dir, nb3, lng.scale, u);
+        ld_link_any<LP>(lng_q, pv, dir, nb3, lng.scale, lng.recon, u);
         ld_spinor<SP>(src, pv, nb3, v);
         mdv_sub(u, v, acc);
     }
@@ -156,7 +156,7 @@ __device__ __forceinline__ void dslash_site_t(const Geom &g, int pv, const LinkS
         for (int k = 0; k < 18; ++k) u[k] = (T)ul[k];
         ld_spinor_as<SP>(src, pv, nf1, v);
         mv_add(u, v, acc);
-        ld_link<LP>(lng_p, pv, dir, i, lng.scale, ul);
+        ld_link_any<LP>(lng_p, pv, dir, i, lng.scale, lng.recon, ul);
 #pragma unroll
         for (int k = 0; k < 18; ++k) u[k] = (T)ul[k];
         ld_spinor_as<SP>(src, pv, nf3, v);
@@ -166,7 +166,7 @@ __device__ __forceinline__ void dslash_site_t(const Geom &g, int pv, const LinkS
         for (int k = 0; k < 18; ++k) u[k] = (T)ul[k];
         ld_spinor_as<SP>(src, pv, nb1, v);
         mdv_sub(u, v, acc);
-        ld_link<LP>(lng_q, pv, dir, nb3, lng.scale, ul);
+        ld_link_any<LP>(lng_q, pv, dir, nb3, lng.scale, lng.recon, ul);
 #pragma unroll
         for (int k = 0; k < 18; ++k) u[k] = (T)ul[k];
         ld_spinor_as<SP>(src, pv, nb3, v);
@@ -203,7 +203,7 @@ __device__ __forceinline__ void dslash_site_mrhs(const Geom &g, int pv, const Li
                 ld_spinor<SP>(src0 + sys[r] * stride, pv, nf1, v);
                 mv_add(u, v, acc[r]);
             }
-        ld_link<LP>(lng_p, pv, dir, i, lng.scale, u);
+        ld_link_any<LP>(lng_p, pv, dir, i, lng.scale, lng.recon, u);
 #pragma unroll
         for (int r = 0; r < R; ++r)
             if (sys[r] >= 0) {
@@ -217,7 +217,7 @@ __device__ __forceinline__ void dslash_site_mrhs(const Geom &g, int pv, const Li
                 ld_spinor<SP>(src0 + sys[r] * stride, pv, nb1, v);
                 mdv_sub(u, v, acc[r]);
             }
-        ld_link<LP>(lng_q, pv, dir, nb3, lng.scale, u);
+        ld_link_any<LP>(lng_q, pv, dir, nb3, lng.scale, lng.recon, u);
 #pragma unroll
         for (int r = 0; r < R; ++r)
             if (sys[r] >= 0) {

@@ -71,7 +71,7 @@ __global__ void links_convert_kernel(Geom g, int pv, LinkSet in, LinkSet out)
     const int rem = t - par * 4 * g.vh;
     const int dir = rem / g.vh, i = rem - dir * g.vh;
     typename Acc<IP>::T u[18];
-    ld_link<IP>(in.par[par], pv, dir, i, in.scale, u);
+    ld_link_any<IP>(in.par[par], pv, dir, i, in.scale, in.recon, u);
     double d[18];
 #pragma unroll
     for (int k = 0; k < 18; ++k) d[k] = (double)u[k];
@@ -87,7 +87,7 @@ __global__ void links_absmax_kernel(Geom g, int pv, LinkSet in, unsigned *out)
         const int rem = t - par * 4 * g.vh;
         const int dir = rem / g.vh, i = rem - dir * g.vh;
         typename Acc<IP>::T u[18];
-        ld_link<IP>(in.par[par], pv, dir, i, in.scale, u);
+        ld_link_any<IP>(in.par[par], pv, dir, i, in.scale, in.recon, u);
 #pragma unroll
         for (int k = 0; k < 18; ++k) m = fmaxf(m, fabsf((float)u[k]));
     }
@@ -102,6 +102,7 @@ cudaError_t links_from_host_record(const Geom &g, const void *d_rec, int rec_pre
     const int pv = pad_sites(g.vh);
     const size_t n = (size_t)2 * g.vh * 72;
     out.scale = 1.f;
+    out.recon = 0;
     if (out_prec == P16) {
         KQ_CUDA_TRY(cudaMemsetAsync(m, 0, sizeof(unsigned), s));
         if (rec_prec == P64)
@@ -155,6 +156,7 @@ cudaError_t links_convert(const Geom &g, const LinkSet &in, int in_prec, LinkSet
 {
     const int pv = pad_sites(g.vh);
     out.scale = 1.f;
+    out.recon = 0;
     if (out_prec == P16) {
         const float am = links_absmax(g, in, in_prec, m, s);
         if (am < 0.f) {
@@ -177,6 +179,112 @@ cudaError_t links_convert(const Geom &g, const LinkSet &in, int in_prec, LinkSet
     }
 #undef KQ_C
     return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------------ compression
+// A link L = s W with W in SU(3) and s real has det L = s^3 and row 2 = conj(row0 x row1) / s.  The check kernel
+// returns the largest |row2 - conj(row0 x row1) / s| / |s| (or a huge value where det L is not real and nonzero);
+// the pack kernel writes rows 0 and 1 and 1/s in the compressed layout of kq_prec.cuh.
+__device__ __forceinline__ double link_scale_from_det(const double u[18], double *det_im)
+{
+    // det = sum_c row0_c * (row1 x row2)_c
+    double dr = 0.0, di = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+        const double xr = (u[6 + 2 * c1] * u[12 + 2 * c2] - u[6 + 2 * c1 + 1] * u[12 + 2 * c2 + 1]) -
+                          (u[6 + 2 * c2] * u[12 + 2 * c1] - u[6 + 2 * c2 + 1] * u[12 + 2 * c1 + 1]);
+        const double xi = (u[6 + 2 * c1] * u[12 + 2 * c2 + 1] + u[6 + 2 * c1 + 1] * u[12 + 2 * c2]) -
+                          (u[6 + 2 * c2] * u[12 + 2 * c1 + 1] + u[6 + 2 * c2 + 1] * u[12 + 2 * c1]);
+        dr += u[2 * c] * xr - u[2 * c + 1] * xi;
+        di += u[2 * c] * xi + u[2 * c + 1] * xr;
+    }
+    *det_im = di;
+    return cbrt(dr);
+}
+
+template <int IP>
+__global__ void links_recon_check_kernel(Geom g, int pv, LinkSet in, double tol, unsigned *out)
+{
+    float m = 0.f;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 8 * g.vh; t += gridDim.x * blockDim.x) {
+        const int par = t / (4 * g.vh);
+        const int rem = t - par * 4 * g.vh;
+        const int dir = rem / g.vh, i = rem - dir * g.vh;
+        typename Acc<IP>::T uf[18];
+        ld_link<IP>(par ? in.par[1] : in.par[0], pv, dir, i, in.scale, uf);
+        double u[18], w[18];
+#pragma unroll
+        for (int k = 0; k < 18; ++k) w[k] = u[k] = (double)uf[k];
+        double di;
+        const double sc = link_scale_from_det(u, &di);
+        float err = 3.0e38f;
+        if (sc != 0.0 && fabs(di) <= tol * fabs(sc * sc * sc)) {
+            rebuild_row2(w, 1.0 / sc);
+            double e = 0.0;
+#pragma unroll
+            for (int k = 12; k < 18; ++k) e = fmax(e, fabs(w[k] - u[k]));
+            err = (float)(e / fabs(sc));
+        }
+        m = fmaxf(m, err);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+template <int IP>
+__global__ void links_recon_pack_kernel(Geom g, int pv, LinkSet in, void *out0, void *out1)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 8 * g.vh) return;
+    const int par = t / (4 * g.vh);
+    const int rem = t - par * 4 * g.vh;
+    const int dir = rem / g.vh, i = rem - dir * g.vh;
+    typename Acc<IP>::T uf[18];
+    ld_link<IP>(par ? in.par[1] : in.par[0], pv, dir, i, in.scale, uf);
+    double u[18];
+#pragma unroll
+    for (int k = 0; k < 18; ++k) u[k] = (double)uf[k];
+    double di;
+    const double sc = link_scale_from_det(u, &di);
+    st_link_recon<IP>(par ? out1 : out0, pv, dir, i, u, 1.0 / sc);
+}
+
+// Compress a full-storage FP64 or FP32 link set in place when every link passes the check (relative
+// reconstruction error below tol); *done reports whether it did.
+cudaError_t links_compress(const Geom &g, LinkSet &lk, int prec, double tol, unsigned *m, cudaStream_t s, bool *done)
+{
+    *done = false;
+    if ((prec != P64 && prec != P32) || lk.recon) return cudaSuccess;
+    const int pv = pad_sites(g.vh);
+    KQ_CUDA_TRY(cudaMemsetAsync(m, 0, sizeof(unsigned), s));
+    if (prec == P64) links_recon_check_kernel<0><<<592, 256, 0, s>>>(g, pv, lk, tol, m);
+    else links_recon_check_kernel<1><<<592, 256, 0, s>>>(g, pv, lk, tol, m);
+    KQ_CUDA_TRY(cudaGetLastError());
+    unsigned h = 0;
+    KQ_CUDA_TRY(cudaMemcpyAsync(&h, m, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    KQ_CUDA_TRY(cudaStreamSynchronize(s));
+    float err;
+    memcpy(&err, &h, sizeof(float));
+    if (!(err <= tol)) return cudaSuccess;
+    const size_t part = (size_t)(prec == P64 ? 104 : 52) * 4 * pv;  // one parity, 4 directions
+    void *tmp = nullptr;
+    KQ_CUDA_TRY(cudaMallocAsync(&tmp, 2 * part, s));
+    char *t0 = static_cast<char *>(tmp);
+    const int threads = 256, blocks = (8 * g.vh + threads - 1) / threads;
+    if (prec == P64) links_recon_pack_kernel<0><<<blocks, threads, 0, s>>>(g, pv, lk, t0, t0 + part);
+    else links_recon_pack_kernel<1><<<blocks, threads, 0, s>>>(g, pv, lk, t0, t0 + part);
+    cudaError_t e = cudaGetLastError();
+    // the compressed parity fields fit in the full-storage regions they replace
+    if (e == cudaSuccess) e = cudaMemcpyAsync(lk.par[0], t0, part, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(lk.par[1], t0 + part, part, cudaMemcpyDeviceToDevice, s);
+    cudaFreeAsync(tmp, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    KQ_CUDA_TRY(e);
+    lk.recon = 1;
+    *done = true;
+    return cudaSuccess;
 }
 
 // ------------------------------------------------------------------------------------------------ spinors

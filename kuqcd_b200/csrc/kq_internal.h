@@ -14,6 +14,10 @@
 //     HALF: [dir][2 x int4 + 1 x int (2 x int16)][site], value = q * scale / 32767          36 B/link
 //   Device links carry the reference kernel's constants: fat_dev = 1/2 * F, long_dev = c3 * L with
 //   c3 = -1/48 (dirac_hisq.cpp:40,464-502), so the dslash is a plain sum of U v and U^dag v products.
+//   Long links that are a real multiple of an SU(3) matrix, L = s W (HISQ's Naik links are products of
+//   reunitarised links), are stored compressed: rows 0 and 1 and 1/s, row 2 = conj(row0 x row1) / s:
+//     FP64: [dir][6 x double2 + 1 x double][site]                                          104 B/link
+//     FP32: [dir][3 x float4 + 1 x float][site]                                              52 B/link
 #pragma once
 #include <cuda_runtime.h>
 #include <cstddef>
@@ -56,6 +60,8 @@ struct SpinorView {
 struct LinkSet {          // one link type (fat or long) in one precision, both parities
     void *par[2];         // device pointer per parity
     float scale;          // HALF only: value = q * scale / 32767
+    int recon;            // FP64 / FP32 only: 1 = two rows + 1/s per link, the third row rebuilt (kq_prec.cuh);
+                          // 0 in a value-initialised context, set by every link writer
 };
 
 struct GaugeDev {
@@ -83,6 +89,10 @@ cudaError_t links_from_host_record(const Geom &g, const void *d_rec, int rec_pre
 cudaError_t links_convert(const Geom &g, const LinkSet &in, int in_prec, LinkSet &out, int out_prec,
                           unsigned *scratch, cudaStream_t s);
 float links_absmax(const Geom &g, const LinkSet &in, int in_prec, unsigned *scratch, cudaStream_t s);
+// store an FP64 / FP32 link set compressed (two rows + 1/s) in place if every link is a real multiple of an SU(3)
+// matrix to relative accuracy tol; *done reports whether it did
+cudaError_t links_compress(const Geom &g, LinkSet &lk, int prec, double tol, unsigned *scratch, cudaStream_t s,
+                           bool *done);
 cudaError_t spinor_from_record(const Geom &g, const void *d_rec, int rec_prec, void *dst, int prec, cudaStream_t s);
 cudaError_t spinor_to_record(const Geom &g, const void *src, int prec, void *d_rec, int rec_prec, cudaStream_t s);
 cudaError_t spinor_convert(const Geom &g, const void *src, int src_prec, void *dst, int dst_prec, cudaStream_t s);

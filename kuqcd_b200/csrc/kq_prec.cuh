@@ -205,4 +205,92 @@ template <> __device__ __forceinline__ void st_link<2>(void *par_base, int pv, i
     reinterpret_cast<int *>(d + (size_t)32 * pv)[i] = pack16(q[16], q[17]);
 }
 
+// ------------------------------------------------------------------------------------------------ compressed links
+// L = s W with W in SU(3) (s real): rows 0 and 1 of L and 1/s are stored; row 2 = conj(row0 x row1) / s.
+// FP64: 6 double2 planes + 1 double plane per direction (104 B per link); FP32: 3 float4 + 1 float (52 B).
+template <typename T>
+__device__ __forceinline__ void rebuild_row2(T u[18], T inv_s)
+{
+    // (a x b)_c = a_{c+1} b_{c+2} - a_{c+2} b_{c+1}; row 2 = conj(a x b) * inv_s with a = row 0, b = row 1
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+        const T ar1 = u[2 * c1], ai1 = u[2 * c1 + 1], ar2 = u[2 * c2], ai2 = u[2 * c2 + 1];
+        const T br1 = u[6 + 2 * c1], bi1 = u[6 + 2 * c1 + 1], br2 = u[6 + 2 * c2], bi2 = u[6 + 2 * c2 + 1];
+        const T re = (ar1 * br2 - ai1 * bi2) - (ar2 * br1 - ai2 * bi1);
+        const T im = (ar1 * bi2 + ai1 * br2) - (ar2 * bi1 + ai2 * br1);
+        u[12 + 2 * c] = re * inv_s;
+        u[12 + 2 * c + 1] = -im * inv_s;
+    }
+}
+
+template <int P>
+__device__ __forceinline__ void ld_link_recon(const void *par_base, int pv, int dir, int i,
+                                              typename Acc<P>::T u[18]);
+
+template <> __device__ __forceinline__ void ld_link_recon<0>(const void *par_base, int pv, int dir, int i, double u[18])
+{
+    const char *d = static_cast<const char *>(par_base) + (size_t)dir * 104 * pv;
+    const double2 *b = reinterpret_cast<const double2 *>(d) + i;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const double2 w = ld_stream(b + (size_t)k * pv);
+        u[2 * k] = w.x;
+        u[2 * k + 1] = w.y;
+    }
+    rebuild_row2(u, __ldcs(reinterpret_cast<const double *>(d + (size_t)96 * pv) + i));
+}
+
+template <> __device__ __forceinline__ void ld_link_recon<1>(const void *par_base, int pv, int dir, int i, float u[18])
+{
+    const char *d = static_cast<const char *>(par_base) + (size_t)dir * 52 * pv;
+    const float4 *b4 = reinterpret_cast<const float4 *>(d) + i;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float4 w = ld_stream(b4 + (size_t)k * pv);
+        u[4 * k] = w.x; u[4 * k + 1] = w.y; u[4 * k + 2] = w.z; u[4 * k + 3] = w.w;
+    }
+    rebuild_row2(u, __ldcs(reinterpret_cast<const float *>(d + (size_t)48 * pv) + i));
+}
+
+template <> __device__ __forceinline__ void ld_link_recon<2>(const void *, int, int, int, float u[18])
+{
+#pragma unroll
+    for (int k = 0; k < 18; ++k) u[k] = 0.f;  // HALF links are never stored compressed
+}
+
+// any storage of a LinkSet: full (recon = 0) or compressed
+template <int P>
+__device__ __forceinline__ void ld_link_any(const void *par_base, int pv, int dir, int i, float scale, int recon,
+                                            typename Acc<P>::T u[18])
+{
+    if (P != 2 && recon) ld_link_recon<P>(par_base, pv, dir, i, u);
+    else ld_link<P>(par_base, pv, dir, i, scale, u);
+}
+
+// store rows 0, 1 and inv_s of one link in the compressed layout
+template <int P>
+__device__ __forceinline__ void st_link_recon(void *par_base, int pv, int dir, int i, const double u[18], double inv_s);
+
+template <> __device__ __forceinline__ void st_link_recon<0>(void *par_base, int pv, int dir, int i, const double u[18],
+                                                             double inv_s)
+{
+    char *d = static_cast<char *>(par_base) + (size_t)dir * 104 * pv;
+    double2 *b = reinterpret_cast<double2 *>(d) + i;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) b[(size_t)k * pv] = make_double2(u[2 * k], u[2 * k + 1]);
+    reinterpret_cast<double *>(d + (size_t)96 * pv)[i] = inv_s;
+}
+
+template <> __device__ __forceinline__ void st_link_recon<1>(void *par_base, int pv, int dir, int i, const double u[18],
+                                                             double inv_s)
+{
+    char *d = static_cast<char *>(par_base) + (size_t)dir * 52 * pv;
+    float4 *b4 = reinterpret_cast<float4 *>(d) + i;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        b4[(size_t)k * pv] = make_float4((float)u[4 * k], (float)u[4 * k + 1], (float)u[4 * k + 2], (float)u[4 * k + 3]);
+    reinterpret_cast<float *>(d + (size_t)48 * pv)[i] = (float)inv_s;
+}
+
 }  // namespace kq

@@ -57,13 +57,13 @@ __device__ __forceinline__ void slab_site(const Geom &g, int pv, const LinkSet &
             ld_link<P>(fat_p, pv, dir, i, fat.scale, u);
             ld_spinor<P>(src, pv, nf1, v);
             mv_add(u, v, acc);
-            ld_link<P>(lng_p, pv, dir, i, lng.scale, u);
+            ld_link_any<P>(lng_p, pv, dir, i, lng.scale, lng.recon, u);
             ld_spinor<P>(src, pv, nf3, v);
             mv_add(u, v, acc);
             ld_link<P>(fat_q, pv, dir, nb1, fat.scale, u);
             ld_spinor<P>(src, pv, nb1, v);
             mdv_sub(u, v, acc);
-            ld_link<P>(lng_q, pv, dir, nb3, lng.scale, u);
+            ld_link_any<P>(lng_q, pv, dir, nb3, lng.scale, lng.recon, u);
             ld_spinor<P>(src, pv, nb3, v);
             mdv_sub(u, v, acc);
         } else {
@@ -71,7 +71,8 @@ __device__ __forceinline__ void slab_site(const Geom &g, int pv, const LinkSet &
 #pragma unroll
             for (int h = 1; h <= 3; h += 2) {
                 const int tt = c.t + h;
-                ld_link<P>(h == 1 ? fat_p : lng_p, pv, 3, i, h == 1 ? fat.scale : lng.scale, u);
+                if (h == 1) ld_link<P>(fat_p, pv, 3, i, fat.scale, u);
+                else ld_link_any<P>(lng_p, pv, 3, i, lng.scale, lng.recon, u);
                 if (tt < lt) ld_spinor<P>(src, pv, i + h * S, v);
                 else ld_spinor<P>(a.ghi, a.pvg, (tt - lt) * S + j, v);
                 mv_add(u, v, acc);
@@ -81,7 +82,8 @@ __device__ __forceinline__ void slab_site(const Geom &g, int pv, const LinkSet &
             for (int h = 1; h <= 3; h += 2) {
                 const int tt = c.t - h;
                 if (tt >= 0) {
-                    ld_link<P>(h == 1 ? fat_q : lng_q, pv, 3, i - h * S, h == 1 ? fat.scale : lng.scale, u);
+                    if (h == 1) ld_link<P>(fat_q, pv, 3, i - h * S, fat.scale, u);
+                    else ld_link_any<P>(lng_q, pv, 3, i - h * S, lng.scale, lng.recon, u);
                     ld_spinor<P>(src, pv, i - h * S, v);
                 } else {
                     ld_link<P>(h == 1 ? a.gfat_q : a.glng_q, a.pvg, 0, (tt + 3) * S + j, 1.f, u);
@@ -139,7 +141,7 @@ __global__ void slab_link_pack_kernel(Geom g, int pv, LinkSet fat, LinkSet lng, 
     for (int q = 0; q < 4; ++q) {
         const LinkSet &L = q < 2 ? fat : lng;
         double u[18];
-        ld_link<0>(q & 1 ? L.par[1] : L.par[0], pv, 3, i, 1.f, u);
+        ld_link_any<0>(q & 1 ? L.par[1] : L.par[0], pv, 3, i, 1.f, L.recon, u);
         st_link<0>(face + q * part_bytes, pvg, 0, k, 1.f, u);
     }
 }

@@ -63,7 +63,7 @@ EXPORTED_SYMBOLS = [
     "kq_kuqcd_init", "kq_kuqcd_load_gaugefield", "kq_kuqcd_solve_multishift", "kq_kuqcd_gauge_free",
     "kq_kuqcd_end", "kq_context_create", "kq_context_destroy", "kq_load_links", "kq_prepare_links",
     "kq_spinor_bytes", "kq_spinor_upload", "kq_spinor_download", "kq_spinor_convert", "kq_dslash", "kq_mdagm",
-    "kq_mdagm_noalloc", "kq_dslash_full", "kq_mdagm_full", "kq_slab_set", "kq_slab_face_bytes",
+    "kq_mdagm_noalloc", "kq_dslash_full", "kq_mdagm_full", "kq_long_links_compressed", "kq_slab_set", "kq_slab_face_bytes",
     "kq_slab_pack_faces", "kq_slab_link_face_bytes", "kq_slab_pack_link_face", "kq_slab_set_link_ghosts",
     "kq_slab_dslash", "kq_field_axpby", "kq_field_dot",
     "kq_solve_multishift", "kq_solve_multishift_device", "kq_true_residuals", "kq_make_links_record",
@@ -119,6 +119,7 @@ def library() -> C.CDLL:
         "kq_mdagm_noalloc": (i, [vp, i, d, vp, vp, i, vp]),
         "kq_dslash_full": (i, [vp, i, vp, vp, vp]),
         "kq_mdagm_full": (i, [vp, i, d, vp, vp, vp, vp]),
+        "kq_long_links_compressed": (i, [vp, i, C.POINTER(i)]),
         "kq_slab_set": (i, [vp, i, i]),
         "kq_slab_face_bytes": (sz, [vp, i]),
         "kq_slab_pack_faces": (i, [vp, i, vp, vp, vp, vp]),
@@ -269,6 +270,12 @@ class Context:
     def mdagm_noalloc(self, prec: int, sigma: float, src, dst, parity: int, stream=None) -> int:
         """kq_mdagm_noalloc: returns the status (callers test the rejection paths)."""
         return library().kq_mdagm_noalloc(self._h, prec, sigma, _ptr(src), _ptr(dst), parity, stream)
+
+    def long_links_compressed(self, prec: int) -> int:
+        """1: long links of prec stored as two rows + 1/s; 0: full storage; -1: not resident."""
+        v = C.c_int()
+        self._chk(library().kq_long_links_compressed(self._h, prec, C.byref(v)), "kq_long_links_compressed")
+        return v.value
 
     def upload_full(self, prec: int, host: np.ndarray, dev, stream=None):
         """Full-lattice host record (even sites then odd sites, V*6 values) -> full-lattice device field."""

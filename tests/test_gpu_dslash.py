@@ -110,3 +110,36 @@ def test_precision_round_trip(cuda):
         # HALF: 16-bit fixed point relative to the per-site maximum
         site_max = np.abs(src.reshape(-1, 6)).max(axis=1, keepdims=True)
         assert np.all(np.abs(back - src).reshape(-1, 6) <= tol * site_max + 1e-300)
+
+
+@pytest.mark.gpu
+def test_long_links_stored_compressed_when_su3_multiples(cuda, monkeypatch):
+    """Long links that are real multiples of SU(3) matrices (the generator's -1/24 U U U, like HISQ's Naik links)
+    are stored as two rows + 1/s in FP64 and FP32; the operator is unchanged to rounding.  Links that are not (here
+    Gaussian noise) keep full storage.  KUQCD_LONG_RECON=0 turns the compression off."""
+    dims = (8, 6, 4, 4)
+    src = np.random.default_rng(8).standard_normal(int(np.prod(dims)) // 2 * 6)
+    ctx, fat, lng = make_ctx(dims)
+    ctx.prepare(K.KUQCD_SINGLE)
+    ctx.prepare(K.KUQCD_HALF)
+    assert ctx.long_links_compressed(K.KUQCD_DOUBLE) == 1
+    assert ctx.long_links_compressed(K.KUQCD_SINGLE) == 1
+    assert ctx.long_links_compressed(K.KUQCD_HALF) == 0
+    ref = O.dslash(dims, fat, lng, src, 1)
+    packed = run_dslash(ctx, K.KUQCD_DOUBLE, src, 1)
+    assert np.abs(packed - ref).max() <= 1e-13 * np.abs(ref).max()
+    monkeypatch.setenv("KUQCD_LONG_RECON", "0")
+    ctx2, _, _ = make_ctx(dims)
+    assert ctx2.long_links_compressed(K.KUQCD_DOUBLE) == 0
+    full = run_dslash(ctx2, K.KUQCD_DOUBLE, src, 1)
+    assert np.abs(full - packed).max() <= 1e-14 * np.abs(full).max()
+    monkeypatch.delenv("KUQCD_LONG_RECON")
+    # not SU(3) multiples: full storage, same operator as the oracle
+    noise = np.random.default_rng(3).standard_normal(lng.size)
+    ctx3 = K.Context(dims)
+    ctx3.load_links(K.KUQCD_FAT_LINK, fat)
+    ctx3.load_links(K.KUQCD_LONG_LINK, noise)
+    assert ctx3.long_links_compressed(K.KUQCD_DOUBLE) == 0
+    ref3 = O.dslash(dims, fat, noise, src, 1)
+    out3 = run_dslash(ctx3, K.KUQCD_DOUBLE, src, 1)
+    assert np.abs(out3 - ref3).max() <= 1e-13 * np.abs(ref3).max()
