@@ -478,10 +478,10 @@ cudaError_t batch_plan(kq_batch *b, int bs, BatchPlan &plan, bool carve_only, si
         for (int k = 1; k < ns; ++k) h.shift[k] = sig[k] - sig[0];
         if (S.param.solver == KQ_SOLVER_MIXED) {
             // the single-system mixed solver's schedule (kq_mixed.cu): stop at 0.7 x target, FP32 from
-            // 0.3 target / 1e-5, HALF from 0.3 target / 1e-3
+            // 0.3 target / 3e-7, HALF from 0.3 target / 1e-3
             const double tgt = S.param.rel_residual > 0 ? S.param.rel_residual : 1e-10;
             h.tol = -0.7 * tgt;  // relative: the init kernel turns it into (0.7 tgt |b|)^2
-            const double r32 = 0.3 * tgt / 1e-5, r16 = 0.3 * tgt / 1e-3;
+            const double r32 = 0.3 * tgt / 3e-7, r16 = 0.3 * tgt / 1e-3;
             h.rho32_2 = r32 * r32;
             h.rho16_2 = prec_from_api(S.param.prec) == P16 ? r16 * r16 : 0.0;
         } else {
