@@ -285,7 +285,7 @@ def run_ours(args):
     peak = peaks.get("hbm_gbs")
     peak_note = "measured" if peak else "fallback"
     peak = peak or 6650.0
-    achieved = dsl[dom]["gbs"]  # SURVEY's compulsory 2400 B per site (18 reals per link)
+    achieved = dsl[dom]["gbs"]  # the compulsory 2400 B per site (18 reals per link)
     storage_gbs = DSLASH_FP64_STORAGE_BYTES[long_recon] * Vh / (dsl[dom]["ms"] * 1e-3) / 1e9
 
     result = None

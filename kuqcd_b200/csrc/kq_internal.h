@@ -97,7 +97,7 @@ cudaError_t spinor_from_record(const Geom &g, const void *d_rec, int rec_prec, v
 cudaError_t spinor_to_record(const Geom &g, const void *src, int prec, void *d_rec, int rec_prec, cudaStream_t s);
 cudaError_t spinor_convert(const Geom &g, const void *src, int src_prec, void *dst, int dst_prec, cudaStream_t s);
 
-// generators (BASELINE field construction, on the device)
+// generators of the synthetic benchmark fields, on the device
 cudaError_t make_links_record(const Geom &g, double eps, uint64_t seed, double *d_fat_rec, double *d_long_rec,
                               cudaStream_t s);
 cudaError_t make_source_record(const Geom &g, int parity, uint64_t seed, double *d_rec, cudaStream_t s);

@@ -45,7 +45,7 @@ int kqo_cgm_f(const int dims[4], const float *fat, const float *lng, int parity,
 double kqo_true_residual_d(const int dims[4], const double *fat, const double *lng, int parity, double sigma,
                            const double *b, const double *x);
 
-/* BASELINE field construction: thin U_mu(x) = exp(i eps H), H traceless Hermitian from seeded Gaussians;
+/* Synthetic benchmark fields: thin U_mu(x) = exp(i eps H), H traceless Hermitian from seeded Gaussians;
  * staggered phases eta folded in; fat = 9/8 eta U; long = -1/24 eta U(x) U(x+mu) U(x+2mu).  Writes the host
  * gauge layout above.  thin may be NULL. */
 void kqo_make_links(const int dims[4], double eps, uint64_t seed, double *fat, double *lng, double *thin);

@@ -1,10 +1,11 @@
-"""ORACLE / TEST INFRASTRUCTURE ONLY — ctypes access to the CPU checkers.
+"""ORACLE / TEST INFRASTRUCTURE ONLY — ctypes access to the CPU reference implementations.
 
 * ``port``: liboracle.so, the plain-C restatement in hisq_oracle.c (always buildable with gcc).
 * ``ref``:  _ref/libkuqcd_ref.so, the unmodified reference KuQCD sources compiled with a single-rank MPI shim
   (oracle/Makefile).  Present when the reference sources were available at build time.
 
-Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs use this module, as the checker.
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs use this module: it is what GPU results are
+compared with, never part of the product path.
 """
 from __future__ import annotations
 
