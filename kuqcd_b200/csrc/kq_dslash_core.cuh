@@ -85,6 +85,50 @@ __device__ __forceinline__ int nbr_index(const Geom &g, const SiteCoord &c, int 
     }
 }
 
+// One link as type T.  HALF links (LP = 2) come back as raw int16 values: a site's fat-link terms are accumulated
+// in units of the fat field's scale, the long-link terms have their spinor multiplied by scale_long / scale_fat
+// (6 products instead of 18 on the link), and the sum is scaled once at the end (fold_scale_*).
+template <int LP, typename T>
+__device__ __forceinline__ void ld_link_fold(const void *base, int pv, int dir, int i, const LinkSet &L, T u[18])
+{
+    if constexpr (LP == 2) {
+        float q[18];
+        ld_link_q16(base, pv, dir, i, q);
+#pragma unroll
+        for (int k = 0; k < 18; ++k) u[k] = (T)q[k];
+    } else {
+        typename Acc<LP>::T w[18];
+        ld_link_any<LP>(base, pv, dir, i, L.scale, L.recon, w);
+#pragma unroll
+        for (int k = 0; k < 18; ++k) u[k] = (T)w[k];
+    }
+}
+
+template <int LP, typename T>
+__device__ __forceinline__ T fold_scale_long(const LinkSet &fat, const LinkSet &lng)
+{
+    return LP == 2 ? (T)(lng.scale / fat.scale) : T(1);
+}
+
+template <int LP, typename T>
+__device__ __forceinline__ void fold_scale_site(const LinkSet &fat, T acc[6])
+{
+    if constexpr (LP == 2) {
+        const T s = (T)(fat.scale * (1.0f / 32767.0f));
+#pragma unroll
+        for (int k = 0; k < 6; ++k) acc[k] *= s;
+    }
+}
+
+template <int LP, typename T>
+__device__ __forceinline__ void fold_long_spinor(T rl, T v[6])
+{
+    if constexpr (LP == 2) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) v[k] *= rl;
+    }
+}
+
 // Accumulation type of a (link precision, spinor precision) pair: double only when both are FP64.
 template <int LP, int SP> struct Acc2 { using T = float; };
 template <> struct Acc2<0, 0> { using T = double; };
@@ -101,6 +145,7 @@ __device__ __forceinline__ void dslash_site2(const Geom &g, int pv, const LinkSe
     // select parity planes without indexing the parameter arrays dynamically (keeps them out of local memory)
     const void *fat_p = p ? fat.par[1] : fat.par[0], *fat_q = p ? fat.par[0] : fat.par[1];
     const void *lng_p = p ? lng.par[1] : lng.par[0], *lng_q = p ? lng.par[0] : lng.par[1];
+    const T rl = fold_scale_long<LP, T>(fat, lng);
 #pragma unroll
     for (int k = 0; k < 6; ++k) acc[k] = T(0);
 #pragma unroll
@@ -110,19 +155,22 @@ __device__ __forceinline__ void dslash_site2(const Geom &g, int pv, const LinkSe
         const int nb1 = nbr_index(g, c, i, dir, -1);
         const int nb3 = nbr_index(g, c, i, dir, -3);
         T u[18], v[6];
-        ld_link<LP>(fat_p, pv, dir, i, fat.scale, u);
+        ld_link_fold<LP>(fat_p, pv, dir, i, fat, u);
         ld_spinor<SP>(src, pv, nf1, v);
         mv_add(u, v, acc);
-        ld_link_any<LP>(lng_p, pv, dir, i, lng.scale, lng.recon, u);
+        ld_link_fold<LP>(lng_p, pv, dir, i, lng, u);
         ld_spinor<SP>(src, pv, nf3, v);
+        fold_long_spinor<LP>(rl, v);
         mv_add(u, v, acc);
-        ld_link<LP>(fat_q, pv, dir, nb1, fat.scale, u);
+        ld_link_fold<LP>(fat_q, pv, dir, nb1, fat, u);
         ld_spinor<SP>(src, pv, nb1, v);
         mdv_sub(u, v, acc);
-        ld_link_any<LP>(lng_q, pv, dir, nb3, lng.scale, lng.recon, u);
+        ld_link_fold<LP>(lng_q, pv, dir, nb3, lng, u);
         ld_spinor<SP>(src, pv, nb3, v);
+        fold_long_spinor<LP>(rl, v);
         mdv_sub(u, v, acc);
     }
+    fold_scale_site<LP>(fat, acc);
 }
 
 template <int P>
@@ -141,6 +189,7 @@ __device__ __forceinline__ void dslash_site_t(const Geom &g, int pv, const LinkS
     const SiteCoord c = site_coord(g, i, p);
     const void *fat_p = p ? fat.par[1] : fat.par[0], *fat_q = p ? fat.par[0] : fat.par[1];
     const void *lng_p = p ? lng.par[1] : lng.par[0], *lng_q = p ? lng.par[0] : lng.par[1];
+    const T rl = fold_scale_long<LP, T>(fat, lng);
 #pragma unroll
     for (int k = 0; k < 6; ++k) acc[k] = T(0);
 #pragma unroll
@@ -149,29 +198,23 @@ __device__ __forceinline__ void dslash_site_t(const Geom &g, int pv, const LinkS
         const int nf3 = nbr_index(g, c, i, dir, 3);
         const int nb1 = nbr_index(g, c, i, dir, -1);
         const int nb3 = nbr_index(g, c, i, dir, -3);
-        typename Acc<LP>::T ul[18];
         T u[18], v[6];
-        ld_link<LP>(fat_p, pv, dir, i, fat.scale, ul);
-#pragma unroll
-        for (int k = 0; k < 18; ++k) u[k] = (T)ul[k];
+        ld_link_fold<LP>(fat_p, pv, dir, i, fat, u);
         ld_spinor_as<SP>(src, pv, nf1, v);
         mv_add(u, v, acc);
-        ld_link_any<LP>(lng_p, pv, dir, i, lng.scale, lng.recon, ul);
-#pragma unroll
-        for (int k = 0; k < 18; ++k) u[k] = (T)ul[k];
+        ld_link_fold<LP>(lng_p, pv, dir, i, lng, u);
         ld_spinor_as<SP>(src, pv, nf3, v);
+        fold_long_spinor<LP>(rl, v);
         mv_add(u, v, acc);
-        ld_link<LP>(fat_q, pv, dir, nb1, fat.scale, ul);
-#pragma unroll
-        for (int k = 0; k < 18; ++k) u[k] = (T)ul[k];
+        ld_link_fold<LP>(fat_q, pv, dir, nb1, fat, u);
         ld_spinor_as<SP>(src, pv, nb1, v);
         mdv_sub(u, v, acc);
-        ld_link_any<LP>(lng_q, pv, dir, nb3, lng.scale, lng.recon, ul);
-#pragma unroll
-        for (int k = 0; k < 18; ++k) u[k] = (T)ul[k];
+        ld_link_fold<LP>(lng_q, pv, dir, nb3, lng, u);
         ld_spinor_as<SP>(src, pv, nb3, v);
+        fold_long_spinor<LP>(rl, v);
         mdv_sub(u, v, acc);
     }
+    fold_scale_site<LP>(fat, acc);
 }
 
 // Multi-RHS form: the links of site i are loaded once and applied to R right-hand sides whose fields are
@@ -185,6 +228,7 @@ __device__ __forceinline__ void dslash_site_mrhs(const Geom &g, int pv, const Li
     const SiteCoord c = site_coord(g, i, p);
     const void *fat_p = p ? fat.par[1] : fat.par[0], *fat_q = p ? fat.par[0] : fat.par[1];
     const void *lng_p = p ? lng.par[1] : lng.par[0], *lng_q = p ? lng.par[0] : lng.par[1];
+    const T rl = fold_scale_long<LP, T>(fat, lng);
 #pragma unroll
     for (int r = 0; r < R; ++r)
 #pragma unroll
@@ -196,35 +240,39 @@ __device__ __forceinline__ void dslash_site_mrhs(const Geom &g, int pv, const Li
         const int nb1 = nbr_index(g, c, i, dir, -1);
         const int nb3 = nbr_index(g, c, i, dir, -3);
         T u[18], v[6];
-        ld_link<LP>(fat_p, pv, dir, i, fat.scale, u);
+        ld_link_fold<LP>(fat_p, pv, dir, i, fat, u);
 #pragma unroll
         for (int r = 0; r < R; ++r)
             if (sys[r] >= 0) {
                 ld_spinor<SP>(src0 + sys[r] * stride, pv, nf1, v);
                 mv_add(u, v, acc[r]);
             }
-        ld_link_any<LP>(lng_p, pv, dir, i, lng.scale, lng.recon, u);
+        ld_link_fold<LP>(lng_p, pv, dir, i, lng, u);
 #pragma unroll
         for (int r = 0; r < R; ++r)
             if (sys[r] >= 0) {
                 ld_spinor<SP>(src0 + sys[r] * stride, pv, nf3, v);
+                fold_long_spinor<LP>(rl, v);
                 mv_add(u, v, acc[r]);
             }
-        ld_link<LP>(fat_q, pv, dir, nb1, fat.scale, u);
+        ld_link_fold<LP>(fat_q, pv, dir, nb1, fat, u);
 #pragma unroll
         for (int r = 0; r < R; ++r)
             if (sys[r] >= 0) {
                 ld_spinor<SP>(src0 + sys[r] * stride, pv, nb1, v);
                 mdv_sub(u, v, acc[r]);
             }
-        ld_link_any<LP>(lng_q, pv, dir, nb3, lng.scale, lng.recon, u);
+        ld_link_fold<LP>(lng_q, pv, dir, nb3, lng, u);
 #pragma unroll
         for (int r = 0; r < R; ++r)
             if (sys[r] >= 0) {
                 ld_spinor<SP>(src0 + sys[r] * stride, pv, nb3, v);
+                fold_long_spinor<LP>(rl, v);
                 mdv_sub(u, v, acc[r]);
             }
     }
+#pragma unroll
+    for (int r = 0; r < R; ++r) fold_scale_site<LP>(fat, acc[r]);
 }
 
 // ------------------------------------------------------------------------------------------------ reductions

@@ -19,8 +19,16 @@ __device__ __forceinline__ int4 ld_stream(const int4 *p) { return __ldcs(p); }
 __device__ __forceinline__ int ld_stream(const int *p) { return __ldcs(p); }
 
 // int16 fixed point: q = rint(v * 32767 / scale)
-__device__ __forceinline__ float lo16(int w) { return (float)(short)(w & 0xffff); }
-__device__ __forceinline__ float hi16(int w) { return (float)(short)((unsigned)w >> 16); }
+// int16 -> float without the int-to-float conversion unit: flipping the sign bit of q gives q + 32768 in
+// [0, 65535]; placed in the mantissa of 2^23 it is the float 2^23 + q + 32768, and subtracting 2^23 + 32768 leaves q
+// exactly (both operands are integers below 2^24).  One logic op and one float add per value, both full rate; the
+// results equal (float)(short) bit for bit.
+__device__ __forceinline__ float i16_to_f(unsigned biased16)
+{
+    return __uint_as_float(0x4B000000u | biased16) - 8421376.0f;  // 8421376 = 2^23 + 32768
+}
+__device__ __forceinline__ float lo16(int w) { return i16_to_f(((unsigned)w & 0xffffu) ^ 0x8000u); }
+__device__ __forceinline__ float hi16(int w) { return i16_to_f(((unsigned)w >> 16) ^ 0x8000u); }
 __device__ __forceinline__ int pack16(float a, float b)
 {
     const int qa = __float2int_rn(a), qb = __float2int_rn(b);
@@ -164,6 +172,24 @@ template <> __device__ __forceinline__ void ld_link<2>(const void *par_base, int
     const int w = ld_stream(reinterpret_cast<const int *>(d + (size_t)32 * pv) + i);
     u[16] = lo16(w) * s;
     u[17] = hi16(w) * s;
+}
+
+// HALF link as raw int16 values (the per-field scale is applied by the caller, once per site)
+__device__ __forceinline__ void ld_link_q16(const void *par_base, int pv, int dir, int i, float u[18])
+{
+    const char *d = static_cast<const char *>(par_base) + (size_t)dir * 36 * pv;
+    const int4 *b4 = reinterpret_cast<const int4 *>(d) + i;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int4 w = ld_stream(b4 + (size_t)k * pv);
+        u[8 * k + 0] = lo16(w.x); u[8 * k + 1] = hi16(w.x);
+        u[8 * k + 2] = lo16(w.y); u[8 * k + 3] = hi16(w.y);
+        u[8 * k + 4] = lo16(w.z); u[8 * k + 5] = hi16(w.z);
+        u[8 * k + 6] = lo16(w.w); u[8 * k + 7] = hi16(w.w);
+    }
+    const int w = ld_stream(reinterpret_cast<const int *>(d + (size_t)32 * pv) + i);
+    u[16] = lo16(w);
+    u[17] = hi16(w);
 }
 
 // store one link (used by the layout-conversion kernels)
