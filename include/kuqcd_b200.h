@@ -148,7 +148,8 @@ typedef struct {
     int host_prec;            /* precision of the host b / x records */
     int max_iter;
     double tol;               /* KQ_SOLVER_CGM: reference stopping rule zeta_k^2 |r|^2 < tol */
-    double rel_residual;      /* KQ_SOLVER_MIXED: per-shift true relative residual target */
+    double rel_residual;      /* KQ_SOLVER_MIXED: per-shift true relative residual target; < 0: absolute target
+                                 |b - A_k x_k|^2 < tol instead (single-system solves) */
 } kq_solve_param;
 
 typedef struct {

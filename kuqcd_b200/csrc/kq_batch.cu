@@ -390,6 +390,10 @@ KQ_API KuQCDStatus kq_batch_add(kq_batch *b, kq_context *ctx, const kq_solve_par
         set_last_error("kq_batch_add: batched systems use KQ_SOLVER_MIXED or KQ_SOLVER_CGM_WINDOWED");
         return KUQCD_ERR_UNSUPPORTED;
     }
+    if (param->solver == KQ_SOLVER_MIXED && param->rel_residual < 0) {
+        set_last_error("kq_batch_add: batched systems take a relative target (rel_residual > 0)");
+        return KUQCD_ERR_INVALID_PARAM;
+    }
     if (ctx->device != b->device) {
         set_last_error("kq_batch_add: context on another device");
         return KUQCD_ERR_INVALID_PARAM;

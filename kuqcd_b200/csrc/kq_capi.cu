@@ -147,6 +147,7 @@ KQ_API void kq_context_destroy(kq_context *ctx)
     for (void *gl : ctx->ghost_links)
         if (gl) cudaFree(gl);
     if (ctx->work) cudaFree(ctx->work);
+    if (ctx->io) cudaFree(ctx->io);
     if (ctx->d_scratch) cudaFree(ctx->d_scratch);
     if (ctx->poll) cudaFreeHost(ctx->poll);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -640,24 +641,53 @@ KQ_API KuQCDStatus kq_solve_multishift(kq_context *ctx, const kq_solve_param *p,
     const size_t vb = spinor_bytes(ctx->g, P64) * halves;  // one (full-lattice or parity) field
     const size_t hvb = spinor_bytes(ctx->g, P64);            // one parity
     const size_t hrec = (size_t)ctx->g.vh * 6 * (hp == P64 ? 8 : 4);  // one parity host record
-    const size_t io = (size_t)vb * (1 + p->num_shift);
-    void *io_buf = nullptr;
-    // the device fields for b and x live outside the solver workspace
-    cudaError_t e = cudaMallocAsync(&io_buf, io, ctx->stream);
-    if (e != cudaSuccess) return status_of(e);
-    void *d_b = io_buf, *d_x = static_cast<char *>(io_buf) + vb;
-    for (int h = 0; h < halves && st == KUQCD_SUCCESS; ++h)
-        st = kq_spinor_upload(ctx, KUQCD_DOUBLE, static_cast<const char *>(host_b) + h * hrec, p->host_prec,
-                              static_cast<char *>(d_b) + h * hvb, nullptr);
-    if (st == KUQCD_SUCCESS) st = kq_solve_multishift_device(ctx, p, d_b, d_x, info);
-    if (st == KUQCD_SUCCESS || st == KUQCD_ERR_UNKNOWN_ERROR)
-        for (int k = 0; k < p->num_shift; ++k)
-            for (int h = 0; h < halves; ++h) {
-                KuQCDStatus s2 = kq_spinor_download(ctx, KUQCD_DOUBLE, static_cast<char *>(d_x) + k * vb + h * hvb,
-                                                    static_cast<char *>(host_x[k]) + h * hrec, p->host_prec, nullptr);
-                if (s2 != KUQCD_SUCCESS) st = s2;
-            }
-    cudaFreeAsync(io_buf, ctx->stream);
+    // one context-owned buffer (kept between calls): b, the solutions, and the host-record staging of all fields
+    const int nrec = p->num_shift * halves;
+    const size_t fields = (size_t)vb * (1 + p->num_shift), need = fields + hrec * (size_t)nrec;
+    if (ctx->io_bytes < need) {
+        cudaStreamSynchronize(ctx->stream);
+        if (ctx->io) cudaFree(ctx->io);
+        ctx->io = nullptr;
+        ctx->io_bytes = 0;
+        cudaError_t ea = cudaMalloc(&ctx->io, need);
+        if (ea != cudaSuccess) {
+            set_last_error(std::string("kq_solve_multishift: ") + cudaGetErrorString(ea));
+            return status_of(ea);
+        }
+        ctx->io_bytes = need;
+    }
+    char *base = static_cast<char *>(ctx->io);
+    void *d_b = base, *d_x = base + vb;
+    char *sg = base + fields;
+    cudaError_t e = cudaSuccess;
+    for (int h = 0; h < halves && e == cudaSuccess; ++h) {
+        e = cudaMemcpyAsync(sg + h * hrec, static_cast<const char *>(host_b) + h * hrec, hrec, cudaMemcpyHostToDevice,
+                            ctx->stream);
+        if (e == cudaSuccess) e = spinor_from_record(ctx->g, sg + h * hrec, hp, static_cast<char *>(d_b) + h * hvb, P64,
+                                                     ctx->stream);
+    }
+    if (e != cudaSuccess) {
+        set_last_error(std::string("kq_solve_multishift: ") + cudaGetErrorString(e));
+        return status_of(e);
+    }
+    st = kq_solve_multishift_device(ctx, p, d_b, d_x, info);
+    if (st == KUQCD_SUCCESS || st == KUQCD_ERR_UNKNOWN_ERROR) {
+        // every solution into host-record layout, then one copy per field and one sync
+        cudaError_t e2 = cudaSuccess;
+        for (int k = 0; k < p->num_shift && e2 == cudaSuccess; ++k)
+            for (int h = 0; h < halves && e2 == cudaSuccess; ++h)
+                e2 = spinor_to_record(ctx->g, static_cast<char *>(d_x) + k * vb + h * hvb, P64,
+                                      sg + (size_t)(k * halves + h) * hrec, hp, ctx->stream);
+        for (int k = 0; k < p->num_shift && e2 == cudaSuccess; ++k)
+            for (int h = 0; h < halves && e2 == cudaSuccess; ++h)
+                e2 = cudaMemcpyAsync(static_cast<char *>(host_x[k]) + h * hrec, sg + (size_t)(k * halves + h) * hrec,
+                                     hrec, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(ctx->stream);
+        if (e2 != cudaSuccess) {
+            set_last_error(std::string("kq_solve_multishift: ") + cudaGetErrorString(e2));
+            st = status_of(e2);
+        }
+    }
     cudaStreamSynchronize(ctx->stream);
     return st;
 }

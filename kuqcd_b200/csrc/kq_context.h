@@ -15,6 +15,9 @@ struct kq_context {
     // solver workspace (grown on demand, never shrunk)
     void *work = nullptr;
     size_t work_bytes = 0;
+    // device fields and host-record staging of kq_solve_multishift (host buffers in and out), grown on demand
+    void *io = nullptr;
+    size_t io_bytes = 0;
     kq::CgmPoll *poll = nullptr;  // pinned host page for state polling
     // t-slab of a domain-decomposed lattice (kq_slab.cu): this context holds local t = 0 .. nt-1 of global
     // t0 = slab_rank * nt; ghost links are the t-direction fat and long links of the 3 slices below t0, per

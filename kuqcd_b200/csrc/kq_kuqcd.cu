@@ -336,12 +336,9 @@ KQ_API KuQCDStatus kq_kuqcd_solve_multishift(void **hp_x, void *hp_b, KuQCDInver
             for (int k = 0; k < param->num_shift; ++k) xs[k] = hp_x[k];
         }
         if (mixed) {
-            double bb = 0;
-            const double *bd = static_cast<const double *>(b);
-            for (size_t e = 0; e < vh * 6; ++e) bb += bd[e] * bd[e];
             sp.solver = KQ_SOLVER_MIXED;
             sp.prec = mixed_half ? KUQCD_HALF : KUQCD_SINGLE;
-            sp.rel_residual = bb > 0 ? std::sqrt(param->tol / bb) : 1e-10;
+            sp.rel_residual = -1.0;  // absolute: |b - A_k x_k|^2 < tol, |b| taken on the device
         }
         kq_solve_info info;
         KuQCDStatus st = kq_solve_multishift(S.ctx, &sp, b, xs.data(), &info);

@@ -425,7 +425,9 @@ cudaError_t mixed_solve(::kq_context *ctx, const kq_solve_param *param, const do
         set_last_error("mixed solver: sloppy precision must be SINGLE or HALF");
         return cudaErrorInvalidValue;
     }
-    const double target = param->rel_residual > 0 ? param->rel_residual : 1e-10;
+    // rel_residual < 0: the absolute target |b - A_k x_k|^2 < tol (the reference's stopping threshold), turned into
+    // a relative one once |b| is known
+    double target = param->rel_residual > 0 ? param->rel_residual : 1e-10;
     // Effective error of the sloppy operators relative to |r| at the switch.  The HALF operator's residual gap grows
     // to ~1e-3 x the residual norm at which it starts (measured on the oracle).  For FP32 the schedule was swept on
     // B200 (32^4 and 48^3 x 96, 12 and 16 shifts, target 1e-10): 1e-5 -> 3e-7 cuts the solve time by 10-11 % with
@@ -483,6 +485,13 @@ cudaError_t mixed_solve(::kq_context *ctx, const kq_solve_param *param, const do
         if (!(bb > 0) || !std::isfinite(bb)) {
             set_last_error("mixed solver: source norm is zero or not finite");
             return cudaErrorInvalidValue;
+        }
+        if (param->rel_residual < 0) {
+            if (!(param->tol > 0)) {
+                set_last_error("mixed solver: an absolute target (rel_residual < 0) needs tol > 0");
+                return cudaErrorInvalidValue;
+            }
+            target = std::sqrt(param->tol / bb);
         }
         MrState hs;
         memset(&hs, 0, sizeof(hs));

@@ -113,3 +113,32 @@ def test_mixed_through_reference_api(cuda, monkeypatch):
     assert st == 0 and it > 0
     for k in range(12):
         assert O.true_residual(dims, fat, lng, 0, ab[k], b, xs[k]) <= 1.2e-10
+
+
+@pytest.mark.gpu
+def test_mixed_absolute_target(cuda):
+    """rel_residual < 0: the reference's absolute threshold |b - A_k x_k|^2 < tol, with |b| taken on the device
+    (the path kuqcd_solve_multishift uses with KUQCD_SOLVER=mixed); it needs tol > 0, and batched systems refuse
+    it."""
+    import torch
+
+    dims = (8, 8, 8, 4)
+    ctx, fat, lng = ctx_for(dims, 0.3, 77)
+    b = 3.0 * O.make_source(dims, 0, 5)
+    sig = list(0.05 ** 2 + np.logspace(-3, 0, 4))
+    tol = (2e-10) ** 2 * float(b @ b)
+    xs, info = ctx.solve(b, sig, parity=0, solver=K.KQ_SOLVER_MIXED, prec=K.KUQCD_HALF, rel_residual=-1.0, tol=tol)
+    assert info.status == 0
+    for k, s in enumerate(sig):
+        r = O.true_residual(dims, fat, lng, 0, s, b, xs[k])
+        assert r <= 2.2e-10, (k, r)
+    with pytest.raises(K.KuQCDError):
+        ctx.solve(b, sig, parity=0, solver=K.KQ_SOLVER_MIXED, prec=K.KUQCD_HALF, rel_residual=-1.0, tol=0.0)
+    bt = K.Batch()
+    vb = ctx.spinor_bytes(K.KUQCD_DOUBLE)
+    d_b = torch.zeros(vb, dtype=torch.uint8, device="cuda")
+    d_x = torch.zeros(4 * vb, dtype=torch.uint8, device="cuda")
+    with pytest.raises(K.KuQCDError):
+        bt.add(ctx, d_b, d_x, sig, solver=K.KQ_SOLVER_MIXED, rel_residual=-1.0, tol=tol)
+    bt.close()
+    ctx.close()
