@@ -82,6 +82,9 @@ static void free_links(::kq_context *ctx, int prec)
 KuQCDStatus status_of(cudaError_t e)
 {
     if (e == cudaSuccess) return KUQCD_SUCCESS;
+    // the error is being reported to the caller now: clear the runtime's per-thread last error, so that a failed
+    // allocation does not resurface in the next launch check of an unrelated call
+    cudaGetLastError();
     if (e == cudaErrorMemoryAllocation) return KUQCD_ERR_NO_MEMORY;
     if (e == cudaErrorInvalidValue) return KUQCD_ERR_INVALID_PARAM;
     return KUQCD_ERR_UNKNOWN_ERROR;

@@ -103,8 +103,11 @@ __global__ void __launch_bounds__(256) cgm_init_kernel(int vh, int pv, const voi
         st->iter = 0;
         st->nupd = 0;
         st->halt = 0;
-        st->status = 0;
-        st->active = 1;
+        // b = 0: x = 0 is the solution (no iteration; the reference would divide 0 by p.Ap = 0);
+        // a non-finite source is a breakdown
+        const bool finite = isfinite(tot);
+        st->status = finite ? 0 : KQ_STATUS_BREAKDOWN;
+        st->active = (finite && tot > 0.0) ? 1 : 0;
     }
 }
 

@@ -482,9 +482,17 @@ cudaError_t mixed_solve(::kq_context *ctx, const kq_solve_param *param, const do
         launches += 1;
         double bb = 0;
         for (double v : h) bb += v;
-        if (!(bb > 0) || !std::isfinite(bb)) {
-            set_last_error("mixed solver: source norm is zero or not finite");
+        if (!std::isfinite(bb)) {
+            set_last_error("mixed solver: the source is not finite");
             return cudaErrorInvalidValue;
+        }
+        if (bb == 0.0) {  // b = 0: every x_k = 0, exactly
+            KQ_CUDA_TRY(cudaMemsetAsync(d_x, 0, vb64 * ns, s));
+            KQ_CUDA_TRY(cudaStreamSynchronize(s));
+            info->iter = 0;
+            info->kernel_launches = launches;
+            for (int k = 0; k < ns; ++k) info->true_residual[k] = 0.0;
+            return cudaSuccess;
         }
         if (param->rel_residual < 0) {
             if (!(param->tol > 0)) {

@@ -70,8 +70,10 @@ __global__ void __launch_bounds__(kBSm) ms_init_kernel(int vh, int pv, const voi
         st->wpos = 0;
         st->nupd = 0;
         st->halt = 0;
-        st->status = 0;
-        st->active = (tot > 0.0) ? 1 : 0;
+        // b = 0: x = 0 is the solution; a non-finite source is a breakdown
+        const bool finite = isfinite(tot);
+        st->status = finite ? 0 : KQ_STATUS_BREAKDOWN;
+        st->active = (finite && tot > 0.0) ? 1 : 0;
     }
 }
 

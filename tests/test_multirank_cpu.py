@@ -96,3 +96,31 @@ def test_bench_reference_arm_under_torchrun_rank0_only():
     assert len(lines) == 1, out.stdout
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] > 0 and d["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def _dead_peer_worker(rank, world, port, out_dir):
+    import datetime
+
+    import torch.distributed as dist
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=5))
+    if rank == 1:
+        return  # leaves between steps, with nothing in flight: never joins the exchange
+    tr = SL.TorchTransport()
+    t = torch.zeros(16, dtype=torch.float64)
+    try:
+        tr.exchange([(t, t.clone())])
+        outcome = "returned"
+    except Exception as exc:  # the process group's timeout ends the wait with an error
+        outcome = "error: " + type(exc).__name__
+    with open(os.path.join(out_dir, "r0.txt"), "w") as f:
+        f.write(outcome)
+
+
+def test_slab_exchange_with_a_dead_peer_fails_with_an_error(tmp_path):
+    """Failure detection on the host: a rank that never joins the halo exchange makes the others' exchange end
+    with an error after the process group's (short) timeout instead of waiting for good."""
+    mp.spawn(_dead_peer_worker, args=(2, free_port(), str(tmp_path)), nprocs=2, join=True)
+    outcome = (tmp_path / "r0.txt").read_text()
+    assert outcome.startswith("error"), outcome
