@@ -504,6 +504,7 @@ static std::mutex g_batch_mu;  // the descriptor table in constant memory is sha
 
 KQ_API KuQCDStatus kq_batch_solve(kq_batch *b, kq_batch_info *out)
 {
+    kq::NvtxRange nvtx_range_("kq_batch_solve");
     if (!b) return KUQCD_ERR_NULL_POINTER;
     std::lock_guard<std::mutex> lk(g_batch_mu);
     if (b->sys.empty()) {

@@ -461,6 +461,7 @@ static KuQCDStatus solve_full(kq_context *ctx, const kq_solve_param *p, const vo
 KQ_API KuQCDStatus kq_solve_multishift_device(kq_context *ctx, const kq_solve_param *p, const void *d_b, void *d_x,
                                               kq_solve_info *info)
 {
+    kq::NvtxRange nvtx_range_("kq_solve_multishift_device");
     KuQCDStatus st = check_solve_param(ctx, p);
     if (st != KUQCD_SUCCESS) return st;
     if (!d_b || !d_x) return KUQCD_ERR_NULL_POINTER;

@@ -126,6 +126,7 @@ struct Fcg {
 KQ_API KuQCDStatus kq_fcg_polish(kq_context *ctx, kq_net *net, const kq_solve_param *param, const void *d_b,
                                  void *d_x, kq_solve_info *info)
 {
+    kq::NvtxRange nvtx_range_("kq_fcg_polish");
     if (!ctx || !param || !param->shifts || !d_b || !d_x) return KUQCD_ERR_NULL_POINTER;
     if (param->num_shift < 1 || param->num_shift > kMaxShift || (param->parity != 0 && param->parity != 1))
         return KUQCD_ERR_INVALID_PARAM;

@@ -25,9 +25,20 @@
 #include <cstdio>
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "kuqcd_b200.h"
 
 namespace kq {
+
+// NVTX range for the host side of a phase (header-only NVTX 3: a no-op unless a profiler is attached), so that
+// traces and ncu's --nvtx filters can pick out solver phases, batched solves and network steps
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 enum Prec { P64 = 0, P32 = 1, P16 = 2 };
 

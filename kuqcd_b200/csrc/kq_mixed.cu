@@ -526,6 +526,7 @@ cudaError_t mixed_solve(::kq_context *ctx, const kq_solve_param *param, const do
         const double rho32 = relax_frac * target / eps32;
         const double rho16 = lp == P16 ? relax_frac * target / eps16 : 0.0;
         if (run_phase1) {
+            NvtxRange nvtx("mixed: relaxed-precision multishift");
             MsResult r1;
             KQ_CUDA_TRY(ms_solve(ctx, cw, param->parity, ns, rs, stop_frac * stop_frac * target * target * bb,
                                  param->max_iter > 0 ? param->max_iter : 100000, rho32, rho16, &r1));
@@ -535,6 +536,7 @@ cudaError_t mixed_solve(::kq_context *ctx, const kq_solve_param *param, const do
     }
 
     // ---- phase 2
+    NvtxRange nvtx2("mixed: FP64 check and refinement");
     KQ_CUDA_TRY(cudaMemsetAsync(mw.xs, 0, vb32 * ns, s));
     KQ_CUDA_TRY(cudaMemsetAsync(mw.p, 0, vb32 * ns, s));
     // opening reliable update of every system: r_k = b - A_k x_k in FP64, p_k = r_k

@@ -276,6 +276,7 @@ int net_apply_launches(const kq_net *n) { return n ? 2 + 2 * n->nl : 0; }
 // d_out = M(d_in) on `parity` (FP64 fields of the context's layout)
 KQ_API KuQCDStatus kq_net_apply(kq_net *n, const void *d_in, void *d_out, int parity)
 {
+    kq::NvtxRange nvtx_range_("kq_net_apply");
     if (!n || !d_in || !d_out) return KUQCD_ERR_NULL_POINTER;
     if (parity != 0 && parity != 1) return KUQCD_ERR_INVALID_PARAM;
     cudaSetDevice(n->ctx->device);
@@ -292,6 +293,7 @@ KQ_API KuQCDStatus kq_net_apply(kq_net *n, const void *d_in, void *d_out, int pa
 KQ_API KuQCDStatus kq_net_train_pair(kq_net *n, const void *d_r, const void *d_e, int parity, double e_norm2,
                                      double *loss)
 {
+    kq::NvtxRange nvtx_range_("kq_net_train_pair");
     if (!n || !d_r || !d_e) return KUQCD_ERR_NULL_POINTER;
     if ((parity != 0 && parity != 1) || !(e_norm2 > 0)) return KUQCD_ERR_INVALID_PARAM;
     cudaSetDevice(n->ctx->device);
