@@ -15,8 +15,9 @@
 // K-major layout, FP32 accumulators in tensor memory, M = 128, N = 16, K = 16 per instruction) for the three
 // colours, and the epilogue reads the accumulators back with tcgen05.ld, one site row per thread.  The adjoint layer
 // (for input gradients) is the same kernel with weights W'[i][o][p'] = conj(W[o][i][p]) and forward/backward hops
-// swapped.  The weight gradient dL/dB = T^T G is a second GEMM over the rows of each tile (mma.sync BF16, FP32
-// accumulate); per-tile partials are summed in a fixed order.
+// swapped.  The weight gradient dL/dB = T^T G is also a tcgen05 GEMM, reading the same gathered tile MN-major
+// (M = k, K = sites) with the accumulator kept in tensor memory across a persistent CTA's tiles; the per-CTA
+// partials are summed in a fixed order.
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -44,15 +45,6 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
     return *reinterpret_cast<uint32_t *>(&h);
 }
 
-__device__ __forceinline__ void mma_bf16(float d[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
-                                         uint32_t b1)
-{
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};\n"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-}
 
 __device__ __forceinline__ float2 ld_act(const float2 *act, int pv, int c, int par, int a, int i)
 {
@@ -117,43 +109,19 @@ __device__ __forceinline__ void gather_paths(const Geom &g, int pv, const LinkSe
 }
 
 // ---------------------------------------------------------------------------------------------------- forward
-// out (C_out channels, both parities) = layer(in); Bt: [NP][KP] BF16 weights (device), built by the host.
-// fault: set when the tensor cores did not signal completion within the wait limit (the tile is then not written).
-constexpr int kNT = 16;                      // N of the tensor-core tile (C_out * 2 padded)
-constexpr uint32_t kTmemCols = 64;           // 3 colours x 16 FP32 accumulator columns, rounded up
-constexpr uint32_t kWaitLimit = 1u << 24;    // mbarrier polls before a tile gives up
-
-template <int CIN, int COUT>
-__global__ void __launch_bounds__(kThr) ptc_forward_kernel(Geom g, int pv, LinkSet fat, const float2 *__restrict__ in,
-                                                           float2 *__restrict__ out, const __nv_bfloat16 *__restrict__ Bt,
-                                                           int swap_paths, int *fault)
+// Gathered inputs of one 128-site tile into shared memory as BF16, one [128 sites x KP] matrix per colour in the
+// canonical core-matrix layout (8 sites x 16 bytes of k per core matrix; k-chunks 128 bytes apart, 8-site groups
+// (KP/8)*128 bytes apart).  The forward GEMM reads it K-major (M = sites), the weight-gradient GEMM MN-major
+// (M = k, K = sites).  Thread t owns site base + t; sites past the end of the lattice are zero rows.
+template <int CIN>
+__device__ __forceinline__ void gather_tile(const Geom &g, int pv, const LinkSet &fat, const float2 *in, int par,
+                                            int base, int t, bool swap_paths, unsigned char *As)
 {
-    constexpr int KP = kpad_of(CIN), NP = npad_of(COUT), KV = CIN * kPaths * 2;
-    constexpr uint32_t A_BYTES = kTile * KP * 2;   // one colour's [128 x KP] operand
-    constexpr uint32_t SBO = (KP / 8) * 128;       // bytes between 8-row groups
-    static_assert(NP <= kNT && KP % 16 == 0, "tile shape");
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char *As = smem_raw;                  // [3][A_BYTES]
-    unsigned char *Bs = As + 3 * A_BYTES;          // [kNT x KP]
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(Bs + kNT * KP * 2);
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
-    const int tiles_per_par = (g.vh + kTile - 1) / kTile;
-    const int par = blockIdx.x / tiles_per_par;
-    const int base = (blockIdx.x - par * tiles_per_par) * kTile;
-    const int t = threadIdx.x, warp = t >> 5;
-    if (warp == 0) umma::tmem_alloc(tslot, kTmemCols);
-    if (t == 0) {
-        umma::mbar_init(mbar, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    for (int e = t; e < kNT * KP; e += kThr) {
-        const int n = e / KP, k = e - n * KP;
-        *reinterpret_cast<__nv_bfloat16 *>(Bs + umma::kmajor_offset(n, k, KP)) =
-            n < NP ? Bt[n * KP + k] : __float2bfloat16_rn(0.f);
-    }
+    constexpr int KP = kpad_of(CIN), KV = CIN * kPaths * 2;
+    constexpr uint32_t A_BYTES = kTile * KP * 2;
     const int i = base + t;
     if (i < g.vh) {
-        gather_paths<CIN>(g, pv, fat, in, par, i, swap_paths != 0, [&](int p, const float (&vals)[3][2 * CIN]) {
+        gather_paths<CIN>(g, pv, fat, in, par, i, swap_paths, [&](int p, const float (&vals)[3][2 * CIN]) {
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
                 unsigned char *row = As + a * A_BYTES;
@@ -186,6 +154,43 @@ __global__ void __launch_bounds__(kThr) ptc_forward_kernel(Geom g, int pv, LinkS
             for (int k = 0; k < KP; k += 8)
                 *reinterpret_cast<uint4 *>(As + a * A_BYTES + umma::kmajor_offset(t, k, KP)) = make_uint4(0, 0, 0, 0);
     }
+}
+
+// out (C_out channels, both parities) = layer(in); Bt: [NP][KP] BF16 weights (device), built by the host.
+// fault: set when the tensor cores did not signal completion within the wait limit (the tile is then not written).
+constexpr int kNT = 16;                      // N of the tensor-core tile (C_out * 2 padded)
+constexpr uint32_t kTmemCols = 64;           // 3 colours x 16 FP32 accumulator columns, rounded up
+constexpr uint32_t kWaitLimit = 1u << 24;    // mbarrier polls before a tile gives up
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kThr) ptc_forward_kernel(Geom g, int pv, LinkSet fat, const float2 *__restrict__ in,
+                                                           float2 *__restrict__ out, const __nv_bfloat16 *__restrict__ Bt,
+                                                           int swap_paths, int *fault)
+{
+    constexpr int KP = kpad_of(CIN), NP = npad_of(COUT);
+    constexpr uint32_t A_BYTES = kTile * KP * 2;   // one colour's [128 x KP] operand
+    constexpr uint32_t SBO = (KP / 8) * 128;       // bytes between 8-row groups
+    static_assert(NP <= kNT && KP % 16 == 0, "tile shape");
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char *As = smem_raw;                  // [3][A_BYTES]
+    unsigned char *Bs = As + 3 * A_BYTES;          // [kNT x KP]
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(Bs + kNT * KP * 2);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
+    const int tiles_per_par = (g.vh + kTile - 1) / kTile;
+    const int par = blockIdx.x / tiles_per_par;
+    const int base = (blockIdx.x - par * tiles_per_par) * kTile;
+    const int t = threadIdx.x, warp = t >> 5;
+    if (warp == 0) umma::tmem_alloc(tslot, kTmemCols);
+    if (t == 0) {
+        umma::mbar_init(mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int e = t; e < kNT * KP; e += kThr) {
+        const int n = e / KP, k = e - n * KP;
+        *reinterpret_cast<__nv_bfloat16 *>(Bs + umma::kmajor_offset(n, k, KP)) =
+            n < NP ? Bt[n * KP + k] : __float2bfloat16_rn(0.f);
+    }
+    gather_tile<CIN>(g, pv, fat, in, par, base, t, swap_paths != 0, As);
     umma::fence_smem_to_async();
     umma::fence_before_sync();
     __syncthreads();
@@ -228,74 +233,110 @@ __global__ void __launch_bounds__(kThr) ptc_forward_kernel(Geom g, int pv, LinkS
 }
 
 // ---------------------------------------------------------------------------------------------------- weight grad
-// partial[tile][k][n] = sum over the tile's rows (sites x colours) of T[row][k] * G[row][n]
-// (swap_paths: T gathered as by the adjoint layer)
+// partial[cta][k][n] = sum over the tiles this CTA visits (tile = blockIdx.x + j * gridDim.x) and over their rows
+// (sites x colours) of T[row][k] * G[row][n]  (swap_paths: T gathered as by the adjoint layer).
+// Persistent: the accumulator D (M = k, N = 16) stays in tensor memory across all of the CTA's tiles.  A is the
+// gathered tile read MN-major (M = k, K = sites); B = G, [site][n] in 8 x 16-byte core matrices, also MN-major.
+// With KP = 144 two M tiles cover k < 256; the rows of D past KP read neighbouring data and are never stored.
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(kThr) ptc_wgrad_kernel(Geom g, int pv, LinkSet fat, const float2 *__restrict__ in,
                                                          const float2 *__restrict__ gout, float *__restrict__ partial,
-                                                         int swap_paths)
+                                                         int swap_paths, int *fault)
 {
-    constexpr int KP = kpad_of(CIN), NP = npad_of(COUT), RS = kTile + 8;
+    constexpr int KP = kpad_of(CIN), NP = npad_of(COUT), MT = (KP + 127) / 128;
+    constexpr uint32_t A_BYTES = kTile * KP * 2, G_BYTES = kTile * kNT * 2;
+    constexpr uint32_t A_GROUP = (KP / 8) * 128, G_GROUP = (kNT / 8) * 128;  // bytes between 8-site groups
+    static_assert(NP <= kNT && MT <= 2, "tile shape");
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __nv_bfloat16 *Tt = reinterpret_cast<__nv_bfloat16 *>(smem_raw);  // [3][KP][RS]
-    __nv_bfloat16 *Gt = Tt + 3 * KP * RS;                             // [3][NP][RS]
-    const int tiles_per_par = (g.vh + kTile - 1) / kTile;
-    const int par = blockIdx.x / tiles_per_par;
-    const int base = (blockIdx.x - par * tiles_per_par) * kTile;
-    const int t = threadIdx.x;
-    const int i = base + t;
-    for (int a = 0; a < 3; ++a)
-        for (int k = 0; k < KP; ++k) Tt[(a * KP + k) * RS + t] = __float2bfloat16_rn(0.f);
-    if (i < g.vh) {
-        gather_paths<CIN>(g, pv, fat, in, par, i, swap_paths != 0, [&](int p, const float (&vals)[3][2 * CIN]) {
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-#pragma unroll
-                for (int j = 0; j < 2 * CIN; ++j)
-                    Tt[(a * KP + p * 2 * CIN + j) * RS + t] = __float2bfloat16_rn(vals[a][j]);
-        });
+    unsigned char *As = smem_raw;             // [3][A_BYTES]
+    unsigned char *Gs = As + 3 * A_BYTES;     // [3][G_BYTES]
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(Gs + 3 * G_BYTES);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
+    const int tiles_per_par = (g.vh + kTile - 1) / kTile, ntiles = 2 * tiles_per_par;
+    const int t = threadIdx.x, warp = t >> 5;
+    if (warp == 0) umma::tmem_alloc(tslot, 32);
+    if (t == 0) {
+        umma::mbar_init(mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int n = 0; n < NP; ++n) {
-            float v = 0.f;
-            const int o = n >> 1;
-            if (i < g.vh && o < COUT) {
-                const float2 w = ld_act(gout, pv, o, par, a, i);
-                v = (n & 1) ? w.y : w.x;
-            }
-            Gt[(a * NP + n) * RS + t] = __float2bfloat16_rn(v);
-        }
+    umma::fence_before_sync();
     __syncthreads();
-    const int warp = t >> 5, lane = t & 31, gq = lane >> 2, tq = lane & 3;
-    float *out = partial + (size_t)blockIdx.x * KP * NP;
-    for (int mt = warp; mt < KP / 16; mt += 4) {
+    umma::fence_after_sync();
+    const uint32_t tbase = *tslot;
+    bool ok = true;
+    int round = 0;
+    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++round) {
+        if (round > 0) {  // the previous tile's MMAs must be done reading shared memory
+            ok = __syncthreads_and(umma::mbar_wait(mbar, (round - 1) & 1, kWaitLimit));
+            if (!ok) break;
+            umma::fence_after_sync();
+        }
+        const int par = tile / tiles_per_par;
+        const int base = (tile - par * tiles_per_par) * kTile;
+        gather_tile<CIN>(g, pv, fat, in, par, base, t, swap_paths != 0, As);
+        const int i = base + t;
 #pragma unroll
-        for (int nt = 0; nt < NP / 8; ++nt) {
-            float d[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int a = 0; a < 3; ++a) {
+            float gv[kNT];
+#pragma unroll
+            for (int o = 0; o < kNT / 2; ++o) {
+                float2 w = make_float2(0.f, 0.f);
+                if (o < COUT && i < g.vh) w = ld_act(gout, pv, o, par, a, i);
+                gv[2 * o] = w.x;
+                gv[2 * o + 1] = w.y;
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint4 w;
+                w.x = pack_bf16(gv[8 * h + 0], gv[8 * h + 1]);
+                w.y = pack_bf16(gv[8 * h + 2], gv[8 * h + 3]);
+                w.z = pack_bf16(gv[8 * h + 4], gv[8 * h + 5]);
+                w.w = pack_bf16(gv[8 * h + 6], gv[8 * h + 7]);
+                *reinterpret_cast<uint4 *>(Gs + a * G_BYTES + (t >> 3) * G_GROUP + h * 128 + (t & 7) * 16) = w;
+            }
+        }
+        umma::fence_smem_to_async();
+        umma::fence_before_sync();
+        __syncthreads();
+        umma::fence_after_sync();
+        if (t == 0) {
+            constexpr uint32_t idesc = umma::idesc_bf16_f32(128, kNT, true, true);
+            const uint32_t a0 = umma::smem_u32(As), b0 = umma::smem_u32(Gs);
 #pragma unroll 1
             for (int a = 0; a < 3; ++a)
 #pragma unroll
-                for (int ks = 0; ks < kTile / 16; ++ks) {
-                    const __nv_bfloat16 *A0 = Tt + (a * KP + mt * 16 + gq) * RS + ks * 16 + 2 * tq;
-                    const __nv_bfloat16 *A1 = A0 + 8 * RS;
-                    const uint32_t a0 = *reinterpret_cast<const uint32_t *>(A0);
-                    const uint32_t a1 = *reinterpret_cast<const uint32_t *>(A1);
-                    const uint32_t a2 = *reinterpret_cast<const uint32_t *>(A0 + 8);
-                    const uint32_t a3 = *reinterpret_cast<const uint32_t *>(A1 + 8);
-                    const __nv_bfloat16 *B0 = Gt + (a * NP + nt * 8 + gq) * RS + ks * 16 + 2 * tq;
-                    const uint32_t b0 = *reinterpret_cast<const uint32_t *>(B0);
-                    const uint32_t b1 = *reinterpret_cast<const uint32_t *>(B0 + 8);
-                    mma_bf16(d, a0, a1, a2, a3, b0, b1);
-                }
-            const int k0 = mt * 16 + gq, n0 = nt * 8 + 2 * tq;
-            out[k0 * NP + n0] = d[0];
-            out[k0 * NP + n0 + 1] = d[1];
-            out[(k0 + 8) * NP + n0] = d[2];
-            out[(k0 + 8) * NP + n0 + 1] = d[3];
+                for (int ks = 0; ks < kTile / 16; ++ks)
+#pragma unroll
+                    for (int mt = 0; mt < MT; ++mt)
+                        umma::mma_bf16(tbase + mt * kNT,
+                                       umma::smem_desc2(a0 + a * A_BYTES + 2 * ks * A_GROUP + mt * 16 * 128, A_GROUP, 128),
+                                       umma::smem_desc2(b0 + a * G_BYTES + 2 * ks * G_GROUP, G_GROUP, 128), idesc,
+                                       (round > 0 || a > 0 || ks > 0) ? 1u : 0u);
+            umma::mma_commit(mbar);
         }
     }
+    if (ok && round > 0) ok = __syncthreads_and(umma::mbar_wait(mbar, (round - 1) & 1, kWaitLimit));
+    if (!ok) {
+        if (t == 0) atomicExch(fault, 1);
+        umma::mbar_wait(mbar, (round - 1) & 1, kWaitLimit);  // a last chance for MMAs in flight
+    }
+    umma::fence_after_sync();
+    float *out = partial + (size_t)blockIdx.x * KP * NP;
+    if (ok) {
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+            float d[16];
+            umma::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + mt * kNT, d);  // lane = row k of this M tile
+            const int k = mt * 128 + warp * 32 + (t & 31);
+            if (k < KP) {
+#pragma unroll
+                for (int n = 0; n < NP; ++n) out[(size_t)k * NP + n] = round > 0 ? d[n] : 0.f;
+            }
+        }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tbase, 32);
 }
 
 // fixed-order sum of the per-tile partials: dB[e] = sum_tile partial[tile][e]
@@ -383,8 +424,11 @@ __global__ void ptc_adam_kernel(float *w, const float *grad, float *m, float *v,
 // ---------------------------------------------------------------------------------------------------- host side
 template <int CIN, int COUT>
 static size_t fwd_smem() { return (size_t)(3 * kTile + kNT) * kpad_of(CIN) * 2 + 16; }
+// operands + barrier words, plus one colour's worth of slack: the MMAs of the second M tile read up to a site
+// group past the last colour's A block, and the slack keeps every operand read inside the allocation whatever the
+// stride order of the descriptor
 template <int CIN, int COUT>
-static size_t wgrad_smem() { return (size_t)3 * (kpad_of(CIN) + npad_of(COUT)) * (kTile + 8) * 2; }
+static size_t wgrad_smem() { return (size_t)3 * kTile * (kpad_of(CIN) + kNT) * 2 + 16 + (size_t)kTile * kpad_of(CIN) * 2; }
 
 // device word the forward kernels set when a tile's tensor-core work did not complete in time
 __device__ int g_ptc_fault;
@@ -438,9 +482,16 @@ static cudaError_t run_wgrad(const Geom &g, const LinkSet &fat, const float2 *in
     const size_t sm = wgrad_smem<CIN, COUT>();
     KQ_CUDA_TRY(cudaFuncSetAttribute(ptc_wgrad_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sm));
-    ptc_wgrad_kernel<CIN, COUT><<<tiles, kThr, sm, s>>>(g, pv, fat, in, gout, partial, swap ? 1 : 0);
+    int *fault = fault_flag();
+    if (!fault) return cudaErrorInvalidDevicePointer;
+    // persistent: one CTA per SM (the operand tiles fill most of shared memory), each accumulating its tiles
+    int dev = 0, nsm = 148;
+    KQ_CUDA_TRY(cudaGetDevice(&dev));
+    KQ_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int ctas = std::max(1, std::min(tiles, nsm));
+    ptc_wgrad_kernel<CIN, COUT><<<ctas, kThr, sm, s>>>(g, pv, fat, in, gout, partial, swap ? 1 : 0, fault);
     const int nelem = kpad_of(CIN) * npad_of(COUT);
-    ptc_reduce_kernel<<<std::min(nelem, 1024), 256, 0, s>>>(partial, tiles, nelem, dB);
+    ptc_reduce_kernel<<<std::min(nelem, 1024), 256, 0, s>>>(partial, ctas, nelem, dB);
     return cudaGetLastError();
 }
 

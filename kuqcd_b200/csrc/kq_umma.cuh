@@ -35,10 +35,21 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t sbo)
            ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
 }
 
-// instruction descriptor of kind::f16: BF16 A and B (both K-major), FP32 accumulator, M x N
-__host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N)
+// shared-memory matrix descriptor with explicit offsets.  K-major: lbo = between K-adjacent core matrices, sbo =
+// between M/N-adjacent ones.  MN-major (no swizzle): sbo = between M/N-adjacent core matrices (each 8 K-rows of
+// 16 bytes = 8 M/N elements), lbo = between K-adjacent ones.
+__device__ __forceinline__ uint64_t smem_desc2(uint32_t saddr, uint32_t lbo, uint32_t sbo)
 {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// instruction descriptor of kind::f16: BF16 A and B, FP32 accumulator, M x N; a_mn / b_mn select the MN-major
+// operand layout (default K-major)
+__host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N, bool a_mn = false, bool b_mn = false)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((a_mn ? 1u : 0u) << 15) | ((b_mn ? 1u : 0u) << 16) |
+           ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
 // tensor-memory allocation of ncols columns (power of two >= 32) by one full warp; the base address is written to
