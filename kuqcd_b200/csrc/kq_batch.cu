@@ -14,13 +14,15 @@
 // single-system mixed solver.
 //
 // Tuning: tile size (threads per CTA) and resident CTAs per SM of the persistent grid are chosen by timing one
-// window of the actual batch (kq_tune.cu), cached on disk.
+// window of the actual batch (kq_tune.cu), cached on disk.  Systems large enough to fill the GPU alone go through
+// the single-system solver instead, concurrently with the batched small ones (kq_batch_solve).
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <string>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "kq_context.h"
@@ -115,9 +117,12 @@ __global__ void __launch_bounds__(BS) bk_init_kernel(const SysDesc *__restrict__
                 }
                 st->maxTerm = st->ns;
                 st->wmax = st->ns;
-                st->iter = st->wpos = st->nupd = st->halt = st->status = 0;
+                st->iter = st->wpos = st->nupd = st->halt = 0;
                 st->mode = 0;
-                st->active = tot > 0.0 ? 1 : 0;
+                // b = 0: x = 0 is the solution; a non-finite source is a breakdown
+                const bool finite = isfinite(tot);
+                st->status = finite ? 0 : KQ_STATUS_BREAKDOWN;
+                st->active = (finite && tot > 0.0) ? 1 : 0;
                 if (!st->active && st->running) atomicSub(st->running, 1);
                 st->ticket[0] = 0;
             }
@@ -127,9 +132,10 @@ __global__ void __launch_bounds__(BS) bk_init_kernel(const SysDesc *__restrict__
 }
 
 // K1: tmp = D p0 for the systems whose operator precision is M (one launch per precision, so that each launch is
-// specialised; systems in the other precisions skip their items)
+// specialised; systems in the other precisions skip their items).  FP64 and HALF get up to 128 registers: at the
+// 85-register cap of three 256-thread CTAs per SM the long-link row rebuild and the HALF decode spill.
 template <int BS, int M>
-__global__ void __launch_bounds__(BS, 768 / BS) bk_dslash1_kernel(const SysDesc *__restrict__ sys,
+__global__ void __launch_bounds__(BS, (M == 1 ? 768 : 512) / BS) bk_dslash1_kernel(const SysDesc *__restrict__ sys,
                                                         const int2 *__restrict__ items, int nitems)
 {
     typedef typename Acc2<M, M>::T T;
@@ -149,7 +155,7 @@ __global__ void __launch_bounds__(BS, 768 / BS) bk_dslash1_kernel(const SysDesc 
 
 // K2: s = sigma0 p0 - D tmp (FP64), <p0, s> -> beta step, for the systems in precision M
 template <int BS, int M>
-__global__ void __launch_bounds__(BS, 768 / BS) bk_dslash2_kernel(const SysDesc *__restrict__ sys,
+__global__ void __launch_bounds__(BS, (M == 1 ? 768 : 512) / BS) bk_dslash2_kernel(const SysDesc *__restrict__ sys,
                                                         const int2 *__restrict__ items, int nitems)
 {
     typedef typename Acc2<M, M>::T T;
@@ -502,27 +508,11 @@ cudaError_t batch_plan(kq_batch *b, int bs, BatchPlan &plan, bool carve_only, si
 
 static std::mutex g_batch_mu;  // the descriptor table in constant memory is shared by all batches
 
-KQ_API KuQCDStatus kq_batch_solve(kq_batch *b, kq_batch_info *out)
+// The batched iterations over every system in b->sys, then each system's FP64 check / refinement.
+static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
 {
-    kq::NvtxRange nvtx_range_("kq_batch_solve");
-    if (!b) return KUQCD_ERR_NULL_POINTER;
-    std::lock_guard<std::mutex> lk(g_batch_mu);
-    if (b->sys.empty()) {
-        set_last_error("kq_batch_solve: empty batch");
-        return KUQCD_ERR_INVALID_PARAM;
-    }
     cudaSetDevice(b->device);
     cudaStream_t s = b->stream;
-    // links the schedules need
-    for (auto &S : b->sys) {
-        const bool mixed = S.param.solver == KQ_SOLVER_MIXED;
-        const int precs[3] = {KUQCD_DOUBLE, KUQCD_SINGLE, KUQCD_HALF};
-        const int need = mixed ? (prec_from_api(S.param.prec) == P16 ? 3 : 2) : 1;
-        for (int p = 0; p < need; ++p) {
-            KuQCDStatus st = kq_prepare_links(S.ctx, precs[p]);
-            if (st != KUQCD_SUCCESS) return st;
-        }
-    }
     int dev_sms = 148;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, b->device);
 
@@ -694,4 +684,93 @@ KQ_API KuQCDStatus kq_batch_solve(kq_batch *b, kq_batch_info *out)
         out->tuned_now = have_tune ? 0 : 1;
     }
     return KUQCD_SUCCESS;
+}
+
+// Systems of at least this many sites per parity fill the GPU on their own, and the single-system solver (kernels
+// specialised for one lattice, no per-item mode checks) runs them faster than the batched kernels (measured on
+// B200: 24^3 x 48 and 32^4 systems 10-16 % faster one after another); smaller systems are batched.  Override with
+// KUQCD_BATCH_LARGE_SITES.
+static int large_sites()
+{
+    const char *e = getenv("KUQCD_BATCH_LARGE_SITES");
+    return e ? atoi(e) : 131072;
+}
+
+KQ_API KuQCDStatus kq_batch_solve(kq_batch *b, kq_batch_info *out)
+{
+    kq::NvtxRange nvtx_range_("kq_batch_solve");
+    if (!b) return KUQCD_ERR_NULL_POINTER;
+    std::lock_guard<std::mutex> lk(g_batch_mu);
+    if (b->sys.empty()) {
+        set_last_error("kq_batch_solve: empty batch");
+        return KUQCD_ERR_INVALID_PARAM;
+    }
+    cudaSetDevice(b->device);
+    // links the schedules need
+    for (auto &S : b->sys) {
+        const bool mixed = S.param.solver == KQ_SOLVER_MIXED;
+        const int precs[3] = {KUQCD_DOUBLE, KUQCD_SINGLE, KUQCD_HALF};
+        const int need = mixed ? (prec_from_api(S.param.prec) == P16 ? 3 : 2) : 1;
+        for (int p = 0; p < need; ++p) {
+            KuQCDStatus st = kq_prepare_links(S.ctx, precs[p]);
+            if (st != KUQCD_SUCCESS) return st;
+        }
+    }
+    const int big = large_sites();
+    std::vector<int> large, small;
+    for (size_t i = 0; i < b->sys.size(); ++i) (b->sys[i].ctx->g.vh >= big ? large : small).push_back((int)i);
+    if (large.empty()) return solve_batched(b, out);
+
+    // the small systems, batched, in a helper thread on the batch's stream; meanwhile the large ones one after
+    // another on their own contexts' streams (the two kinds of work overlap on the GPU)
+    std::vector<BatchSystem> all;
+    all.swap(b->sys);
+    for (int i : small) b->sys.push_back(all[i]);
+    kq_batch_info bi;
+    memset(&bi, 0, sizeof(bi));
+    KuQCDStatus st_small = KUQCD_SUCCESS;
+    std::string err_small;
+    std::thread th;
+    if (!b->sys.empty())
+        th = std::thread([&]() {
+            st_small = solve_batched(b, &bi);
+            if (st_small != KUQCD_SUCCESS) err_small = last_error();
+        });
+    KuQCDStatus st_large = KUQCD_SUCCESS;
+    double worst = 0.0;
+    int maxit = 0, refined = 0;
+    long long launches = 0;
+    for (int i : large) {
+        BatchSystem &S = all[i];
+        kq_solve_param p = S.param;
+        p.shifts = S.shifts.data();
+        const KuQCDStatus st = kq_solve_multishift_device(S.ctx, &p, S.d_b, S.d_x, &S.info);
+        if (st != KUQCD_SUCCESS && st_large == KUQCD_SUCCESS) st_large = st;
+        maxit = std::max(maxit, S.info.iter);
+        launches += S.info.kernel_launches;
+        if (S.info.iter_refine > 0) ++refined;
+        if (S.param.solver == KQ_SOLVER_MIXED)
+            for (int k = 0; k < S.param.num_shift; ++k) worst = std::max(worst, S.info.true_residual[k]);
+    }
+    if (th.joinable()) th.join();
+    for (size_t j = 0; j < small.size(); ++j) all[small[j]].info = b->sys[j].info;
+    b->sys.swap(all);
+    cudaSetDevice(b->device);
+    if (out) {
+        memset(out, 0, sizeof(*out));
+        out->num_systems = (int)b->sys.size();
+        out->iterations = std::max(maxit, bi.iterations);
+        out->batched_seconds = bi.batched_seconds;
+        out->kernel_launches = launches + bi.kernel_launches;
+        out->tile = bi.tile;
+        out->ctas_per_sm = bi.ctas_per_sm;
+        out->max_true_residual = std::max(worst, bi.max_true_residual);
+        out->refined_systems = refined + bi.refined_systems;
+        out->tuned_now = bi.tuned_now;
+    }
+    if (st_small != KUQCD_SUCCESS) {
+        set_last_error(err_small);
+        return st_small;
+    }
+    return st_large;
 }
