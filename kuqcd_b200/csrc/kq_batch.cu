@@ -185,9 +185,9 @@ __global__ void __launch_bounds__(BS, (M == 1 ? 768 : 512) / BS) bk_dslash2_kern
         if (threadIdx.x == 0) d.partials[w.y] = dot;
         if (tile_ticket_last(&st->ticket[1], d.ntiles)) {
             const double tot = tile_partials_sum(d.partials, d.ntiles, sm);
-            if (threadIdx.x == 0) {
-                ms_step_beta(st, tot);
-                st->ticket[1] = 0;
+            if (threadIdx.x < 32) {
+                ms_step_beta(st, __shfl_sync(0xffffffffu, tot, 0));
+                if (threadIdx.x == 0) st->ticket[1] = 0;
             }
         }
         __syncthreads();
@@ -227,9 +227,9 @@ __global__ void __launch_bounds__(BS) bk_r_kernel(const SysDesc *__restrict__ sy
         if (threadIdx.x == 0) d.partials[w.y] = nn;
         if (tile_ticket_last(&st->ticket[2], d.ntiles)) {
             const double tot = tile_partials_sum(d.partials, d.ntiles, sm);
-            if (threadIdx.x == 0) {
-                ms_step_alpha(st, tot);
-                st->ticket[2] = 0;
+            if (threadIdx.x < 32) {
+                ms_step_alpha(st, __shfl_sync(0xffffffffu, tot, 0));
+                if (threadIdx.x == 0) st->ticket[2] = 0;
             }
         }
         __syncthreads();

@@ -24,48 +24,77 @@ cudaError_t launch_dslash_gated(const Geom &g, const GaugeDev &gd, int lp, int s
                                 int dst_parity, const int *gate, cudaStream_t s);
 
 // ------------------------------------------------------------------------------------------------ scalar steps
+// Run by the 32 lanes of one warp (of the last block of the reduction), lane l owning shifts l and l + 32: shared
+// scalars are read by every lane before any lane writes, per-shift values only by their owner, so the result is
+// that of the reference's sequential loops (inverter_cgm.cpp:48-57, 58-60, 64-77) with the loads overlapped.
 __device__ void cgm_step_beta(CgmState *st, double pAp)
 {
-    st->pAp = pAp;
-    const double B0 = -st->rNorm2 / pAp;
-    if (!(pAp != 0.0) || !isfinite(B0)) {  // breakdown: zero or non-finite p.Ap
-        st->status = KQ_STATUS_BREAKDOWN;
-        st->active = 0;
-        st->halt = 1;
+    const int lane = threadIdx.x & 31;
+    const double rNorm2 = st->rNorm2, Bm1 = st->Bm1, a0 = st->a[0];
+    const int mt = st->maxTerm;
+    const double B0 = -rNorm2 / pAp;
+    const bool bad = !(pAp != 0.0) || !isfinite(B0);  // breakdown: zero or non-finite p.Ap
+    __syncwarp();
+    if (bad) {
+        if (lane == 0) {
+            st->pAp = pAp;
+            st->status = KQ_STATUS_BREAKDOWN;
+            st->active = 0;
+            st->halt = 1;
+        }
         return;
     }
-    st->B[0] = B0;
-    const double Bm1 = st->Bm1, a0 = st->a[0];
-    for (int j = 1; j < st->maxTerm; ++j) {
-        const double rr1 = Bm1 * st->Zm1[j] /
-                           (B0 * a0 * (st->Zm1[j] - st->Z[j]) + st->Zm1[j] * Bm1 * (1.0 - st->shift[j] * B0));
-        st->Zm1[j] = st->Z[j];
-        st->Z[j] = st->Z[j] * rr1;
+#pragma unroll 1
+    for (int j = 1 + lane; j < mt; j += 32) {
+        const double zm1 = st->Zm1[j], z = st->Z[j], sh = st->shift[j];
+        const double rr1 = Bm1 * zm1 / (B0 * a0 * (zm1 - z) + zm1 * Bm1 * (1.0 - sh * B0));
+        st->Zm1[j] = z;
+        st->Z[j] = z * rr1;
         st->B[j] = B0 * rr1;
     }
-    st->Bm1 = B0;
+    __syncwarp();
+    if (lane == 0) {
+        st->pAp = pAp;
+        st->B[0] = B0;
+        st->Bm1 = B0;
+    }
 }
 
 __device__ void cgm_step_alpha(CgmState *st, double lambda2)
 {
-    st->lambda2 = lambda2;
-    st->a[0] = lambda2 / st->rNorm2;
-    st->rNorm2 = lambda2;
-    for (int j = 1; j < st->maxTerm; ++j) st->a[j] = st->a[0] * st->Z[j] * st->B[j] / (st->Zm1[j] * st->B[0]);
-    st->nupd = st->maxTerm;
-    int mt = st->maxTerm;
-    double lambda;
-    do {
-        lambda = st->Z[mt - 1] * st->Z[mt - 1] * lambda2;
-        if (lambda < st->tol) mt--;
-    } while (mt > 0 && lambda < st->tol);
-    st->maxTerm = mt;
-    st->iter += 1;
-    if (!isfinite(lambda2)) {
-        st->status = KQ_STATUS_BREAKDOWN;
-        st->halt = 1;
+    const int lane = threadIdx.x & 31;
+    const double rNorm2 = st->rNorm2, B0 = st->B[0], tol = st->tol;
+    const int mt0 = st->maxTerm, halt0 = st->halt;
+    const double a0 = lambda2 / rNorm2;
+    __syncwarp();
+    int mt = 0;
+#pragma unroll
+    for (int base = 0; base < kMaxShift; base += 32) {
+        const int k = base + lane;
+        bool keep = false;
+        if (k < mt0) {
+            const double z = st->Z[k];
+            if (k > 0) st->a[k] = a0 * z * st->B[k] / (st->Zm1[k] * B0);
+            keep = !(z * z * lambda2 < tol);  // converged shifts drop from the top
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (m) mt = base + 32 - __clz((int)m);
     }
-    st->active = (mt > 0 && st->iter < st->max_iter && !st->halt) ? 1 : 0;
+    __syncwarp();
+    if (lane == 0) {
+        st->lambda2 = lambda2;
+        st->a[0] = a0;
+        st->rNorm2 = lambda2;
+        st->nupd = mt0;
+        st->maxTerm = mt;
+        st->iter += 1;
+        const bool finite = isfinite(lambda2);
+        if (!finite) {
+            st->status = KQ_STATUS_BREAKDOWN;
+            st->halt = 1;
+        }
+        st->active = (mt > 0 && st->iter < st->max_iter && !halt0 && finite) ? 1 : 0;
+    }
 }
 
 // ------------------------------------------------------------------------------------------------ kernels
@@ -135,7 +164,7 @@ __global__ void __launch_bounds__(256) cgm_dslash2_kernel(Geom g, int pv, LinkSe
         for (int k = 0; k < 6; ++k) dot += (double)pv6[k] * (double)acc[k];
     }
     double tot;
-    if (grid_sum_last(dot, partials, &st->ticket, sm, &tot)) cgm_step_beta(st, tot);
+    if (grid_sum_last_warp(dot, partials, &st->ticket, sm, &tot)) cgm_step_beta(st, tot);
 }
 
 // r += B0 s ; |r|^2
@@ -161,7 +190,7 @@ __global__ void __launch_bounds__(256) cgm_r_kernel(int vh, int pv, void *__rest
         st_spinor<P>(r, pv, i, rv);
     }
     double tot;
-    if (grid_sum_last(nn, partials, &st->ticket, sm, &tot)) cgm_step_alpha(st, tot);
+    if (grid_sum_last_warp(nn, partials, &st->ticket, sm, &tot)) cgm_step_alpha(st, tot);
 }
 
 // x_k -= B_k p_k ; p_k = Z_k r + a_k p_k   for k < nupd

@@ -294,10 +294,10 @@ __device__ __forceinline__ double block_sum(double v, double *smem32)
     return v;  // valid in thread 0
 }
 
-// Publish this block's partial sum; returns true in exactly one thread of the last block to arrive, after which
-// *total holds the fixed-order sum of all partials.  Every block calls this unconditionally.
-__device__ __forceinline__ bool grid_sum_last(double v, double *partials, unsigned *ticket, double *smem32,
-                                              double *total)
+// Publish this block's partial sum; returns true in the 32 threads of warp 0 of the last block to arrive, each
+// holding in *total the fixed-order sum of all partials.  Every block calls this unconditionally.
+__device__ __forceinline__ bool grid_sum_last_warp(double v, double *partials, unsigned *ticket, double *smem32,
+                                                   double *total)
 {
     __shared__ bool am_last;
     v = block_sum(v, smem32);
@@ -313,12 +313,17 @@ __device__ __forceinline__ bool grid_sum_last(double v, double *partials, unsign
     double s = 0.0;
     for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) s += *((volatile double *)partials + b);
     s = block_sum(s, smem32);
-    if (threadIdx.x == 0) {
-        *total = s;
-        *ticket = 0u;
-        return true;
-    }
-    return false;
+    if (threadIdx.x >= 32) return false;
+    *total = __shfl_sync(0xffffffffu, s, 0);
+    if (threadIdx.x == 0) *ticket = 0u;
+    return true;
+}
+
+// As grid_sum_last_warp, but true in exactly one thread (thread 0 of the last block).
+__device__ __forceinline__ bool grid_sum_last(double v, double *partials, unsigned *ticket, double *smem32,
+                                              double *total)
+{
+    return grid_sum_last_warp(v, partials, ticket, smem32, total) && threadIdx.x == 0;
 }
 
 }  // namespace kq

@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(kBSm) ms_dslash2_kernel(Geom g, int pv, LinkSe
         st_spinor<0>(s, pv, i, sv);
     }
     double tot;
-    if (grid_sum_last(dot, partials, &st->ticket[1], sm, &tot)) ms_step_beta(st, tot);
+    if (grid_sum_last_warp(dot, partials, &st->ticket[1], sm, &tot)) ms_step_beta(st, tot);
 }
 
 // K3: r^(i) = r^(i-1) + B0 s into the ring ; |r|^2
@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(kBSm) ms_r_kernel(int vh, int pv, char *ring, 
         st_spinor<0>(rout, pv, i, rv);
     }
     double tot;
-    if (grid_sum_last(nn, partials, &st->ticket[2], sm, &tot)) ms_step_alpha(st, tot);
+    if (grid_sum_last_warp(nn, partials, &st->ticket[2], sm, &tot)) ms_step_alpha(st, tot);
 }
 
 // K4: p0 = r^(i) + a0 p0

@@ -94,3 +94,32 @@ def test_batch_argument_checks(cuda):
     with pytest.raises(K.KuQCDError):
         batch.add(ctx, d, d, [0.1])
     batch.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("large_sites", [256, 1])
+def test_batch_with_large_systems_on_the_single_system_solver(cuda, tmp_path, monkeypatch, large_sites):
+    """Systems of at least KUQCD_BATCH_LARGE_SITES sites per parity go through the single-system solver while the
+    rest are batched (256: two of each kind, overlapping on the GPU; 1: every system on its own); each system still
+    reaches its target and reports its own status and iterations."""
+    monkeypatch.setenv("KUQCD_TUNE_CACHE", str(tmp_path / "tune.txt"))
+    monkeypatch.setenv("KUQCD_BATCH_LARGE_SITES", str(large_sites))
+    batch = K.Batch()
+    keep = []
+    for dims, eps, mass, ns, parity, seed in SYSTEMS:
+        ctx, fat, lng, b, d_b, vb = build(dims, eps, seed, parity)
+        sig = list(mass * mass + np.logspace(-4, 0, ns))
+        d_x = torch.zeros(vb * ns, dtype=torch.uint8, device="cuda")
+        batch.add(ctx, d_b, d_x, sig, parity=parity, solver=K.KQ_SOLVER_MIXED, prec=K.KUQCD_HALF,
+                  rel_residual=1e-10, tol=(1e-10) ** 2 * float(b @ b))
+        keep.append((ctx, fat, lng, b, d_x, vb, sig, parity, dims))
+    info = batch.solve()
+    assert info.num_systems == len(SYSTEMS) and info.iterations > 0
+    for i, (ctx, fat, lng, b, d_x, vb, sig, parity, dims) in enumerate(keep):
+        si = batch.system_info(i)
+        assert si.status == 0 and si.iter > 0, i
+        for k, s in enumerate(sig):
+            xk = ctx.download(K.KUQCD_DOUBLE, d_x[k * vb:(k + 1) * vb])
+            r = O.true_residual(dims, fat, lng, parity, s, b, xk)
+            assert r <= 1.2e-10, (i, k, r)
+    batch.close()
