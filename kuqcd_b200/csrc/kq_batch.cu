@@ -272,7 +272,8 @@ __global__ void __launch_bounds__(BS) bk_window_kernel(const SysDesc *__restrict
         const SysDesc &d = c_sys[w.x];
         MsState *st = d.st;
         const int n = st->wpos, kmax = st->wmax;
-        if (n == 0) continue;  // uniform per system: nothing happened in this window
+        // uniform per system: apply a full window, or a partial one once the system has stopped
+        if (n == 0 || (n < kWin && st->active)) continue;
         __syncthreads();
         for (int t = threadIdx.x; t < kmax; t += BS) {
             sc[t] = st->c[t];
@@ -307,7 +308,7 @@ static void enqueue_batch_init(const SysDesc *d, const int2 *items, int nitems, 
 template <int BS>
 static void enqueue_batch_chunk(const SysDesc *d, const int2 *items, int nitems, int grid, cudaStream_t s)
 {
-    for (int it = 0; it < kWin; ++it) {
+    for (int it = 0; it < kChunk; ++it) {
         bk_dslash1_kernel<BS, 0><<<grid, BS, 0, s>>>(d, items, nitems);
         bk_dslash1_kernel<BS, 1><<<grid, BS, 0, s>>>(d, items, nitems);
         bk_dslash1_kernel<BS, 2><<<grid, BS, 0, s>>>(d, items, nitems);
@@ -589,7 +590,7 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
             err = cudaGraphLaunch(exec, s);
             if (err != cudaSuccess) break;
             ++chunks;
-            *launches += 8 * kWin + 1;  // two dslash steps x three precisions + r + p0 per iteration, + window
+            *launches += 8 * kChunk + 1;  // two dslash steps x three precisions + r + p0 per iteration, + window
             if (chunks > 1000000) break;
         }
         cudaEventRecord(e1, s);

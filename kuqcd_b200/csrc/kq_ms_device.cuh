@@ -136,7 +136,7 @@ __device__ __forceinline__ void ms_step_alpha(MsState *st, double lambda2)
     }
 }
 
-// Windowed shift update of one site, one colour component at a time (keeps 8 ring values in registers, not 48):
+// Windowed shift update of one site, one colour component at a time (keeps W ring values in registers, not 6 W):
 //   p_k <- c_k p_k + sum_l d_kl r_l ,  x_k <- x_k + e_k p_k + sum_l f_kl r_l   for k < kmax.
 // Window position l (0-based) holds r^(i0+l+1) in ring slot (l+1) % W; positions >= n are unused (zero weight).
 // FP64 spinor fields are three double2 planes of pv sites (kq_prec.cuh).

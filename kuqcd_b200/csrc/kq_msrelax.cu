@@ -18,7 +18,9 @@
 //
 // Kernels per iteration: K1 tmp = D p0;  K2 s = sigma0 p0 - D tmp, <p0,s> (beta step + x coefficients);
 // K3 r <- r + B0 s into the ring, |r|^2 (alpha step + p coefficients + shift dropping);  K4 p0 <- r + a0 p0.
-// Every W iterations: K5 the windowed shift update.  One CUDA graph per operator precision, W iterations each.
+// One CUDA graph per operator precision, kChunk iterations each followed by K5, the windowed shift update, which
+// applies the window once it is full (W = 2 kChunk iterations) or the solve has stopped, and otherwise returns at
+// once.  The window sets the shift-update traffic, the chunk the granularity of the precision switches.
 #include <cmath>
 #include <cstdlib>
 #include <vector>
@@ -169,26 +171,27 @@ __global__ void __launch_bounds__(kBSm) ms_window_kernel(int vh, int pv, const c
                                                          char *x0, MsState *st)
 {
     __shared__ double sc[kMaxShift], se[kMaxShift], sd[kMaxShift][kWin], sf[kMaxShift][kWin];
-    __shared__ int nw, km;
+    __shared__ int nw, km, act;
     if (threadIdx.x == 0) {
         nw = st->wpos;
         km = st->wmax;
+        act = st->active;
     }
     __syncthreads();
     const int n = nw, kmax = km;
-    if (n > 0) {
-        for (int t = threadIdx.x; t < kmax; t += kBSm) {
-            sc[t] = st->c[t];
-            se[t] = st->e[t];
-            for (int l = 0; l < kWin; ++l) {
-                sd[t][l] = st->d[t][l];
-                sf[t][l] = st->f[t][l];
-            }
+    // every block reads the same wpos / active (the reset below comes after all blocks have arrived)
+    if (n == 0 || (n < kWin && act)) return;  // window not full and the solve still iterating
+    for (int t = threadIdx.x; t < kmax; t += kBSm) {
+        sc[t] = st->c[t];
+        se[t] = st->e[t];
+        for (int l = 0; l < kWin; ++l) {
+            sd[t][l] = st->d[t][l];
+            sf[t][l] = st->f[t][l];
         }
-        __syncthreads();
-        const int i = blockIdx.x * kBSm + threadIdx.x;
-        if (i < vh) window_update_site(ring, vb, pv, i, n, kmax, sc, se, sd, sf, pw0, x0);
     }
+    __syncthreads();
+    const int i = blockIdx.x * kBSm + threadIdx.x;
+    if (i < vh) window_update_site(ring, vb, pv, i, n, kmax, sc, se, sd, sf, pw0, x0);
     // last block resets the window
     __shared__ bool last;
     __syncthreads();
@@ -208,7 +211,7 @@ template <int LP, int SO>
 static void enqueue_ms_chunk(const Geom &g, const GaugeDev &gd, const MsBuffers &w, int parity, cudaStream_t s)
 {
     const int pv = pad_sites(g.vh), nb = (g.vh + kBSm - 1) / kBSm;
-    for (int it = 0; it < kWin; ++it) {
+    for (int it = 0; it < kChunk; ++it) {
         ms_dslash1_kernel<LP, SO><<<nb, kBSm, 0, s>>>(g, pv, gd.fat[LP], gd.lng[LP], w.p0, w.tmp, 1 - parity, w.st);
         ms_dslash2_kernel<LP, SO><<<nb, kBSm, 0, s>>>(g, pv, gd.fat[LP], gd.lng[LP], w.tmp, w.p0, w.s, parity, w.st,
                                                       w.partials);
@@ -302,8 +305,8 @@ cudaError_t ms_solve(::kq_context *ctx, const MsBuffers &w, int parity, int ns, 
         err = cudaGraphLaunch(exec[m], s);
         if (err != cudaSuccess) break;
         chunks[m] += 1;
-        launches += 4 * kWin + 1;
-        if (chunks[0] + chunks[1] + chunks[2] > max_iter / kWin + 2) break;
+        launches += 4 * kChunk + 1;
+        if (chunks[0] + chunks[1] + chunks[2] > max_iter / kChunk + 2) break;
     }
     for (auto &x : exec)
         if (x) cudaGraphExecDestroy(x);

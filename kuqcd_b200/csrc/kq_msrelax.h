@@ -4,7 +4,8 @@
 
 namespace kq {
 
-constexpr int kWin = 8;  // iterations per shift-update window (ring of residuals)
+constexpr int kWin = 16;   // iterations per shift-update window (ring of residuals)
+constexpr int kChunk = 8;  // iterations per CUDA graph: the host picks the operator precision between chunks
 
 struct MsState {
     int iter, maxTerm, active, wpos;  // polled
@@ -40,7 +41,7 @@ struct MsBuffers {
 struct MsResult {
     int iter, status;
     long long launches;
-    int chunks[3];  // windows run with FP64 / FP32 / HALF operators
+    int chunks[3];  // chunks of kChunk iterations run with FP64 / FP32 / HALF operators
 };
 
 void ms_layout(Carve &c, const Geom &g, int ns, const void *d_b, void *d_x, MsBuffers &w);
