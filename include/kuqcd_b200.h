@@ -161,10 +161,14 @@ typedef struct {
     double seconds;           /* device time of the solve */
     long long kernel_launches;/* kernels the solve enqueued (graph nodes included) */
     double sloppy_residual;   /* KQ_SOLVER_MIXED: largest true relative residual after the sloppy multishift */
+    int copies_during_solve;  /* kq_solve_multishift: solutions whose copy to the host began before the solve ended */
 } kq_solve_info;
 
 /* Host b (Vh*6 values of host_prec; V*6 for KQ_PARITY_FULL) -> host x[k].  Copies in, solves on the device,
- * copies out. */
+ * copies out.  With page-locked x buffers (cudaHostAlloc / cudaHostRegister) and a parity solve, each solution is
+ * copied out as soon as the solver has finished with it (a shift that converges early), on a second stream, while
+ * the solve continues; a solution that the refinement changes afterwards is copied again.  The call returns after
+ * every copy has completed. */
 KuQCDStatus kq_solve_multishift(kq_context *ctx, const kq_solve_param *param, const void *host_b,
                                 void *const *host_x, kq_solve_info *info);
 /* Same with device fields in FP64 (d_b: one field; d_x: num_shift fields, kq_spinor_bytes(ctx, 8) apart; twice

@@ -153,6 +153,12 @@ KQ_API void kq_context_destroy(kq_context *ctx)
     if (ctx->io) cudaFree(ctx->io);
     if (ctx->d_scratch) cudaFree(ctx->d_scratch);
     if (ctx->poll) cudaFreeHost(ctx->poll);
+    if (ctx->copy_stream) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        cudaStreamDestroy(ctx->copy_stream);
+    }
+    if (ctx->copy_ready) cudaEventDestroy(ctx->copy_ready);
+    if (ctx->copy_done) cudaEventDestroy(ctx->copy_done);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -627,6 +633,59 @@ static KuQCDStatus solve_full(kq_context *ctx, const kq_solve_param *p, const vo
     return st;
 }
 
+// Solutions into pinned host buffers leave while the solve goes on: the solver reports each solution once it is
+// final (kq_context::solution_ready), and it is converted to the host record on the solver's stream and copied on
+// a second stream, so only the copies of the last shifts to converge remain after the solve.  A solution that a
+// later phase changes is reported again and copied again.  Pageable buffers are copied after the solve: a copy into
+// pageable memory holds the calling thread, which would delay the solver's next launches.
+struct SolutionCopy {
+    char *d_x;
+    size_t vb;  // device solutions, vb apart
+    char *sg;
+    size_t hrec;  // host-record staging, one slot per solution
+    int hp;
+    void *const *host_x;
+    std::vector<char> sent;
+    cudaError_t err;
+};
+
+static void copy_solution(kq_context *ctx, int k, void *user)
+{
+    auto *c = static_cast<SolutionCopy *>(user);
+    if (c->err != cudaSuccess) return;
+    cudaError_t e = cudaSuccess;
+    // a staging slot is rewritten only after the copy that read it has completed
+    if (c->sent[k]) e = cudaStreamWaitEvent(ctx->stream, ctx->copy_done, 0);
+    if (e == cudaSuccess)
+        e = spinor_to_record(ctx->g, c->d_x + k * c->vb, P64, c->sg + k * c->hrec, c->hp, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->copy_ready, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_stream, ctx->copy_ready, 0);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c->host_x[k], c->sg + k * c->hrec, c->hrec, cudaMemcpyDeviceToHost, ctx->copy_stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->copy_done, ctx->copy_stream);
+    c->sent[k] = 1;
+    c->err = e;
+}
+
+static bool host_pinned(const void *ptr)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+static cudaError_t ensure_copy_stream(kq_context *ctx)
+{
+    cudaError_t e = cudaSuccess;
+    if (!ctx->copy_stream) e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !ctx->copy_ready) e = cudaEventCreateWithFlags(&ctx->copy_ready, cudaEventDisableTiming);
+    if (e == cudaSuccess && !ctx->copy_done) e = cudaEventCreateWithFlags(&ctx->copy_done, cudaEventDisableTiming);
+    return e;
+}
+
 KQ_API KuQCDStatus kq_solve_multishift(kq_context *ctx, const kq_solve_param *p, const void *host_b,
                                        void *const *host_x, kq_solve_info *info)
 {
@@ -674,8 +733,33 @@ KQ_API KuQCDStatus kq_solve_multishift(kq_context *ctx, const kq_solve_param *p,
         set_last_error(std::string("kq_solve_multishift: ") + cudaGetErrorString(e));
         return status_of(e);
     }
+    bool overlap = halves == 1;
+    for (int k = 0; k < p->num_shift && overlap; ++k) overlap = host_pinned(host_x[k]);
+    if (overlap && ensure_copy_stream(ctx) != cudaSuccess) {
+        cudaGetLastError();
+        overlap = false;
+    }
+    SolutionCopy cp{static_cast<char *>(d_x), vb, sg, hrec, hp, host_x, std::vector<char>(p->num_shift, 0),
+                    cudaSuccess};
+    if (overlap) {
+        ctx->solution_ready = copy_solution;
+        ctx->solution_ready_user = &cp;
+    }
     st = kq_solve_multishift_device(ctx, p, d_b, d_x, info);
-    if (st == KUQCD_SUCCESS || st == KUQCD_ERR_UNKNOWN_ERROR) {
+    ctx->solution_ready = nullptr;
+    ctx->solution_ready_user = nullptr;
+    if (info) info->copies_during_solve = (int)std::count(cp.sent.begin(), cp.sent.end(), 1);
+    if (overlap && (st == KUQCD_SUCCESS || st == KUQCD_ERR_UNKNOWN_ERROR)) {
+        // the solutions not reported during the solve
+        for (int k = 0; k < p->num_shift; ++k)
+            if (!cp.sent[k]) copy_solution(ctx, k, &cp);
+        cudaError_t e2 = cp.err;
+        if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(ctx->copy_stream);
+        if (e2 != cudaSuccess) {
+            set_last_error(std::string("kq_solve_multishift: ") + cudaGetErrorString(e2));
+            st = status_of(e2);
+        }
+    } else if (st == KUQCD_SUCCESS || st == KUQCD_ERR_UNKNOWN_ERROR) {
         // every solution into host-record layout, then one copy per field and one sync
         cudaError_t e2 = cudaSuccess;
         for (int k = 0; k < p->num_shift && e2 == cudaSuccess; ++k)
@@ -692,6 +776,8 @@ KQ_API KuQCDStatus kq_solve_multishift(kq_context *ctx, const kq_solve_param *p,
             st = status_of(e2);
         }
     }
+    // no copy into the caller's buffers may still be running when this returns
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
     cudaStreamSynchronize(ctx->stream);
     return st;
 }

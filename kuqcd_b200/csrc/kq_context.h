@@ -25,6 +25,15 @@ struct kq_context {
     int slab_rank = -1, slab_nranks = 0;
     void *ghost_links[2] = {nullptr, nullptr};
     bool have_ghost[2] = {false, false};
+    // Solution notification of a parity solve (set by kq_solve_multishift for the duration of one call): the
+    // solvers call solution_ready(ctx, k, user) on the host thread once solution k of their d_x holds the value it
+    // will be returned with, and again if a later phase changes it.  Work it enqueues on `stream` runs after
+    // everything the solver enqueued so far.
+    void (*solution_ready)(kq_context *ctx, int k, void *user) = nullptr;
+    void *solution_ready_user = nullptr;
+    // copies of solutions to the host that overlap the rest of the solve (created on first use)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t copy_ready = nullptr, copy_done = nullptr;
 };
 
 namespace kq {

@@ -589,6 +589,10 @@ cudaError_t mixed_solve(::kq_context *ctx, const kq_solve_param *param, const do
         worst0 = std::max(worst0, hs.res0[k]);
     }
     info->sloppy_residual = worst0;
+    // the refinement changed the solutions of the systems it iterated on
+    if (ctx->solution_ready)
+        for (int k = 0; k < ns; ++k)
+            if (hs.sys_iter[k] > 0) ctx->solution_ready(ctx, k, ctx->solution_ready_user);
     return cudaSuccess;
 }
 

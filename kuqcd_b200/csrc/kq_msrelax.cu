@@ -16,11 +16,19 @@
 //    at |r| < rho32 |b| and to HALF links (16-bit temporary) at |r| < rho16 |b|; all vectors and scalars stay FP64.
 //    With rho = 0 the solver is the plain FP64 multishift CG with windowed updates.
 //
-// Kernels per iteration: K1 tmp = D p0;  K2 s = sigma0 p0 - D tmp, <p0,s> (beta step + x coefficients);
-// K3 r <- r + B0 s into the ring, |r|^2 (alpha step + p coefficients + shift dropping);  K4 p0 <- r + a0 p0.
-// One CUDA graph per operator precision, kChunk iterations each followed by K5, the windowed shift update, which
+// 3. Three kernels per iteration.  The operator is A = sigma0 - D_pq D_qp with D_pq = -D_qp^dag (the backward hops
+//    apply the adjoints of the same stored links), so <p, A p> = sigma0 |p|^2 + |D_qp p|^2: the beta step can run
+//    at the end of the first dslash, and the second dslash applies r <- r + B0 s directly, never storing s
+//    (inverter_cgm.cpp:45-50 forms s, then <p, s>, then r).  In FP64 the two forms of <p, A p> agree to rounding;
+//    with a 16-bit temporary the step length uses |D p|^2 before the temporary is rounded (relative 3e-5), while
+//    the residual update uses the operator actually applied, so the recurrence stays exact.
+//
+// Kernels per iteration: K1 tmp = D p0, |tmp|^2 (beta step + x coefficients);  K2 r <- r + B0 (sigma0 p0 - D tmp)
+// into the ring, |r|^2 (alpha step + p coefficients + shift dropping);  K3 p0 <- r + a0 p0, |p0|^2.
+// One CUDA graph per operator precision, kChunk iterations each followed by K4, the windowed shift update, which
 // applies the window once it is full (W = 2 kChunk iterations) or the solve has stopped, and otherwise returns at
 // once.  The window sets the shift-update traffic, the chunk the granularity of the precision switches.
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <vector>
@@ -59,6 +67,7 @@ __global__ void __launch_bounds__(kBSm) ms_init_kernel(int vh, int pv, const voi
     if (grid_sum_last(nn, partials, &st->ticket[0], sm, &tot)) {
         st->rNorm2 = tot;
         st->bnorm2 = tot;
+        st->pp = tot;  // p0 = b
         st->Bm1 = 1.0;
         for (int k = 0; k < st->ns; ++k) {
             st->a[k] = 0.0;
@@ -79,52 +88,36 @@ __global__ void __launch_bounds__(kBSm) ms_init_kernel(int vh, int pv, const voi
     }
 }
 
-// K1: tmp = D p0 (p0 FP64; links LP; tmp stored in SO)
+// K1: tmp = D p0 (p0 FP64; links LP; tmp stored in SO); |tmp|^2, then the beta step with
+// <p0, A p0> = sigma0 |p0|^2 + |tmp|^2
 template <int LP, int SO>
 __global__ void __launch_bounds__(kBSm) ms_dslash1_kernel(Geom g, int pv, LinkSet fat, LinkSet lng,
                                                           const void *__restrict__ p0, void *__restrict__ tmp, int q,
-                                                          const MsState *st)
-{
-    if (st->active == 0) return;
-    const int i = blockIdx.x * kBSm + threadIdx.x;
-    if (i >= g.vh) return;
-    typedef typename Acc2<LP, LP>::T T;
-    T acc[6];
-    dslash_site_t<LP, 0, T>(g, pv, fat, lng, p0, q, i, acc);
-    st_spinor_as<SO>(tmp, pv, i, acc);
-}
-
-// K2: s = sigma0 p0 - D tmp (tmp stored in SI, links LP) in FP64 ; pAp
-template <int LP, int SI>
-__global__ void __launch_bounds__(kBSm) ms_dslash2_kernel(Geom g, int pv, LinkSet fat, LinkSet lng,
-                                                          const void *__restrict__ tmp, const void *__restrict__ p0,
-                                                          void *__restrict__ s, int p, MsState *st, double *partials)
+                                                          MsState *st, double *partials)
 {
     if (st->active == 0) return;
     __shared__ double sm[32];
     const int i = blockIdx.x * kBSm + threadIdx.x;
-    double dot = 0.0;
+    double tt = 0.0;
     if (i < g.vh) {
         typedef typename Acc2<LP, LP>::T T;
         T acc[6];
-        dslash_site_t<LP, SI, T>(g, pv, fat, lng, tmp, p, i, acc);
-        double pv6[6], sv[6];
-        ld_spinor<0>(p0, pv, i, pv6);
-        const double sig = st->shift[0];
+        dslash_site_t<LP, 0, T>(g, pv, fat, lng, p0, q, i, acc);
+        st_spinor_as<SO>(tmp, pv, i, acc);
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            sv[k] = sig * pv6[k] - (double)acc[k];
-            dot += pv6[k] * sv[k];
-        }
-        st_spinor<0>(s, pv, i, sv);
+        for (int k = 0; k < 6; ++k) tt += (double)acc[k] * (double)acc[k];
     }
     double tot;
-    if (grid_sum_last_warp(dot, partials, &st->ticket[1], sm, &tot)) ms_step_beta(st, tot);
+    if (grid_sum_last_warp(tt, partials, &st->ticket[1], sm, &tot)) ms_step_beta(st, st->shift[0] * st->pp + tot);
 }
 
-// K3: r^(i) = r^(i-1) + B0 s into the ring ; |r|^2
-__global__ void __launch_bounds__(kBSm) ms_r_kernel(int vh, int pv, char *ring, size_t vb, const void *__restrict__ s,
-                                                    MsState *st, double *partials)
+// K2: s = sigma0 p0 - D tmp (tmp stored in SI, links LP; s stays in registers); r^(i+1) = r^(i) + B0 s into the
+// ring; |r|^2, then the alpha step
+template <int LP, int SI>
+__global__ void __launch_bounds__(kBSm) ms_dslash2_kernel(Geom g, int pv, LinkSet fat, LinkSet lng,
+                                                          const void *__restrict__ tmp, const void *__restrict__ p0,
+                                                          char *ring, size_t vb, int p, MsState *st,
+                                                          double *partials)
 {
     if (st->active == 0) return;
     __shared__ double sm[32];
@@ -133,14 +126,17 @@ __global__ void __launch_bounds__(kBSm) ms_r_kernel(int vh, int pv, char *ring, 
     char *rout = ring + (size_t)((it + 1) % kWin) * vb;
     const int i = blockIdx.x * kBSm + threadIdx.x;
     double nn = 0.0;
-    if (i < vh) {
-        double rv[6], sv[6];
+    if (i < g.vh) {
+        typedef typename Acc2<LP, LP>::T T;
+        T acc[6];
+        dslash_site_t<LP, SI, T>(g, pv, fat, lng, tmp, p, i, acc);
+        double pv6[6], rv[6];
+        ld_spinor<0>(p0, pv, i, pv6);
         ld_spinor<0>(rin, pv, i, rv);
-        ld_spinor<0>(s, pv, i, sv);
-        const double b0 = st->B[0];
+        const double sig = st->shift[0], b0 = st->B[0];
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
-            rv[k] += b0 * sv[k];
+            rv[k] += b0 * (sig * pv6[k] - (double)acc[k]);
             nn += rv[k] * rv[k];
         }
         st_spinor<0>(rout, pv, i, rv);
@@ -149,24 +145,32 @@ __global__ void __launch_bounds__(kBSm) ms_r_kernel(int vh, int pv, char *ring, 
     if (grid_sum_last_warp(nn, partials, &st->ticket[2], sm, &tot)) ms_step_alpha(st, tot);
 }
 
-// K4: p0 = r^(i) + a0 p0
+// K3: p0 = r^(i) + a0 p0 ; |p0|^2 for the next beta step
 __global__ void __launch_bounds__(kBSm) ms_p0_kernel(int vh, int pv, const char *ring, size_t vb, void *p0,
-                                                     const MsState *st)
+                                                     MsState *st, double *partials)
 {
     if (st->active == 0) return;
+    __shared__ double sm[32];
     const int i = blockIdx.x * kBSm + threadIdx.x;
-    if (i >= vh) return;
-    const char *r = ring + (size_t)(st->iter % kWin) * vb;
-    double rv[6], pv6[6];
-    ld_spinor<0>(r, pv, i, rv);
-    ld_spinor<0>(p0, pv, i, pv6);
-    const double a0 = st->a[0];
+    double pp = 0.0;
+    if (i < vh) {
+        const char *r = ring + (size_t)(st->iter % kWin) * vb;
+        double rv[6], pv6[6];
+        ld_spinor<0>(r, pv, i, rv);
+        ld_spinor<0>(p0, pv, i, pv6);
+        const double a0 = st->a[0];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) pv6[k] = rv[k] + a0 * pv6[k];
-    st_spinor<0>(p0, pv, i, pv6);
+        for (int k = 0; k < 6; ++k) {
+            pv6[k] = rv[k] + a0 * pv6[k];
+            pp += pv6[k] * pv6[k];
+        }
+        st_spinor<0>(p0, pv, i, pv6);
+    }
+    double tot;
+    if (grid_sum_last(pp, partials, &st->ticket[3], sm, &tot)) st->pp = tot;
 }
 
-// K5: windowed shift update p_k <- c_k p_k + sum_l d_kl r_l ; x_k <- x_k + e_k p_k + sum_l f_kl r_l
+// K4: windowed shift update p_k <- c_k p_k + sum_l d_kl r_l ; x_k <- x_k + e_k p_k + sum_l f_kl r_l
 __global__ void __launch_bounds__(kBSm) ms_window_kernel(int vh, int pv, const char *ring, size_t vb, char *pw0,
                                                          char *x0, MsState *st)
 {
@@ -212,11 +216,11 @@ static void enqueue_ms_chunk(const Geom &g, const GaugeDev &gd, const MsBuffers 
 {
     const int pv = pad_sites(g.vh), nb = (g.vh + kBSm - 1) / kBSm;
     for (int it = 0; it < kChunk; ++it) {
-        ms_dslash1_kernel<LP, SO><<<nb, kBSm, 0, s>>>(g, pv, gd.fat[LP], gd.lng[LP], w.p0, w.tmp, 1 - parity, w.st);
-        ms_dslash2_kernel<LP, SO><<<nb, kBSm, 0, s>>>(g, pv, gd.fat[LP], gd.lng[LP], w.tmp, w.p0, w.s, parity, w.st,
+        ms_dslash1_kernel<LP, SO><<<nb, kBSm, 0, s>>>(g, pv, gd.fat[LP], gd.lng[LP], w.p0, w.tmp, 1 - parity, w.st,
                                                       w.partials);
-        ms_r_kernel<<<nb, kBSm, 0, s>>>(g.vh, pv, (char *)w.ring, w.vb, w.s, w.st, w.partials);
-        ms_p0_kernel<<<nb, kBSm, 0, s>>>(g.vh, pv, (const char *)w.ring, w.vb, w.p0, w.st);
+        ms_dslash2_kernel<LP, SO><<<nb, kBSm, 0, s>>>(g, pv, gd.fat[LP], gd.lng[LP], w.tmp, w.p0, (char *)w.ring,
+                                                      w.vb, parity, w.st, w.partials);
+        ms_p0_kernel<<<nb, kBSm, 0, s>>>(g.vh, pv, (const char *)w.ring, w.vb, w.p0, w.st, w.partials);
     }
     ms_window_kernel<<<nb, kBSm, 0, s>>>(g.vh, pv, (const char *)w.ring, w.vb, (char *)w.pw, (char *)w.x, w.st);
 }
@@ -237,7 +241,6 @@ void ms_layout(Carve &c, const Geom &g, int ns, const void *d_b, void *d_x, MsBu
     w.b = d_b;
     w.x = d_x;
     w.p0 = c.take(vb);
-    w.s = c.take(vb);
     w.tmp = c.take(vb);  // big enough for any temporary precision
     w.ring = c.take(vb * kWin);
     w.pw = c.take(vb * ns);
@@ -294,18 +297,32 @@ cudaError_t ms_solve(::kq_context *ctx, const MsBuffers &w, int parity, int ns, 
     MsPoll *poll = reinterpret_cast<MsPoll *>(ctx->poll);
     cudaError_t err = cudaSuccess;
     int chunks[3] = {0, 0, 0};
+    // Shifts k >= final_from have been reported final.  A shift dropped from the iteration (k >= maxTerm) receives
+    // its last update in the next window flush; once the window is flushed (wpos = 0), x_k no longer changes.
+    int final_from = ns;
+    auto report = [&](int mt) {
+        if (ctx->solution_ready)
+            for (int k = final_from - 1; k >= mt; --k) ctx->solution_ready(ctx, k, ctx->solution_ready_user);
+        final_from = std::min(final_from, mt);
+    };
     for (;;) {
         err = cudaMemcpyAsync(poll, w.st, sizeof(MsPoll), cudaMemcpyDeviceToHost, s);
         if (err == cudaSuccess) err = cudaStreamSynchronize(s);
-        if (err != cudaSuccess || !poll->active) break;
+        if (err != cudaSuccess) break;
+        if (!poll->active) {
+            if (poll->wpos == 0) report(0);  // stopped, last window flushed: every x_k is final
+            break;
+        }
+        const int mt = poll->maxTerm, flushed = poll->wpos == 0;
         const double rel2 = poll->rNorm2 / poll->bnorm2;
         int m = 0;
         if (use16 && rel2 < rho16 * rho16) m = 2;
         else if (use32 && rel2 < rho32 * rho32) m = 1;
         err = cudaGraphLaunch(exec[m], s);
         if (err != cudaSuccess) break;
+        if (flushed) report(mt);  // the work it enqueues runs behind this chunk
         chunks[m] += 1;
-        launches += 4 * kChunk + 1;
+        launches += 3 * kChunk + 1;
         if (chunks[0] + chunks[1] + chunks[2] > max_iter / kChunk + 2) break;
     }
     for (auto &x : exec)

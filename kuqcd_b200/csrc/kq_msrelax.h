@@ -12,9 +12,10 @@ struct MsState {
     double rNorm2, bnorm2;            // polled
     int ns, max_iter, status, halt;
     int nupd, wmax, pad0, pad1;
-    unsigned ticket[3], pad2;
+    unsigned ticket[4];
     double tol;
     double Bm1, pAp, lambda2;
+    double pp;  // |p0|^2 (single-system solver: the beta step takes <p0, A p0> = sigma0 |p0|^2 + |D p0|^2)
     double shift[kMaxShift];  // reference semantics: shift[0] absolute, shift[j] = sigma_j - sigma_0
     double a[kMaxShift], B[kMaxShift], Z[kMaxShift], Zm1[kMaxShift];
     double c[kMaxShift], e[kMaxShift];           // p_k, x_k coefficients of p_k at the window start
@@ -32,7 +33,7 @@ struct MsPoll {
 struct MsBuffers {
     const void *b;  // FP64 source
     void *x;        // ns FP64 solutions, vb apart
-    void *p0, *s, *tmp, *ring, *pw;
+    void *p0, *tmp, *ring, *pw;
     size_t vb;
     double *partials;
     MsState *st;

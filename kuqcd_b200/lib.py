@@ -55,7 +55,7 @@ class SolveParam(C.Structure):
 class SolveInfo(C.Structure):
     _fields_ = [("iter", C.c_int), ("iter_refine", C.c_int), ("status", C.c_int), ("num_shift", C.c_int),
                 ("true_residual", C.c_double * 64), ("seconds", C.c_double), ("kernel_launches", C.c_longlong),
-                ("sloppy_residual", C.c_double)]
+                ("sloppy_residual", C.c_double), ("copies_during_solve", C.c_int)]
 
 
 # every symbol include/*.h declares for the C ABI (checked by the CPU test suite)
@@ -307,15 +307,25 @@ class Context:
         return p, sh
 
     def solve(self, b: np.ndarray, shifts, parity=0, solver=KQ_SOLVER_CGM, prec=KUQCD_DOUBLE, max_iter=10000,
-              tol=0.0, rel_residual=1e-10, shift_mode=1):
-        """Host b -> list of host x (dtype of b).  shift_mode 1: absolute shifts, 0: reference semantics."""
+              tol=0.0, rel_residual=1e-10, shift_mode=1, pinned=False):
+        """Host b -> list of host x (dtype of b).  shift_mode 1: absolute shifts, 0: reference semantics.
+        pinned: pass page-locked host buffers (the library then copies each solution out while the solve goes on)."""
         b = np.ascontiguousarray(b)
-        xs = [np.zeros_like(b) for _ in shifts]
+        if pinned:
+            import torch
+            tb = torch.from_numpy(b).pin_memory()
+            tx = [torch.zeros(b.shape, dtype=tb.dtype).pin_memory() for _ in shifts]
+            bp, xptrs = C.c_void_p(tb.data_ptr()), [t.data_ptr() for t in tx]
+        else:
+            xs = [np.zeros_like(b) for _ in shifts]
+            bp, xptrs = _ptr(b), [x.ctypes.data for x in xs]
         p, keep = self._param(shifts, parity, solver, prec, _np_prec(b), max_iter, tol, rel_residual, shift_mode)
         info = SolveInfo()
-        xp = (C.c_void_p * len(xs))(*[x.ctypes.data for x in xs])
-        st = library().kq_solve_multishift(self._h, C.byref(p), _ptr(b), xp, C.byref(info))
+        xp = (C.c_void_p * len(xptrs))(*xptrs)
+        st = library().kq_solve_multishift(self._h, C.byref(p), bp, xp, C.byref(info))
         self._chk(st, "kq_solve_multishift")
+        if pinned:
+            xs = [t.numpy().copy() for t in tx]
         return xs, info
 
     def solve_device(self, d_b, d_x, shifts, parity=0, solver=KQ_SOLVER_CGM, prec=KUQCD_DOUBLE, max_iter=10000,

@@ -41,7 +41,7 @@ def test_mixed_8x4_config_reaches_1e10(cuda, sloppy, parity):
 @pytest.mark.gpu
 @pytest.mark.parametrize("dims", [(8, 8, 8, 8), (6, 4, 4, 6), (4, 4, 4, 1)])
 def test_windowed_cgm_matches_classic(cuda, dims):
-    """KQ_SOLVER_CGM_WINDOWED runs the CGM recurrences with shift updates deferred over windows of 8 iterations:
+    """KQ_SOLVER_CGM_WINDOWED runs the CGM recurrences with shift updates deferred over windows of 16 iterations:
     same iteration count as the classic kernel order and the same solutions up to rounding."""
     ctx, fat, lng = ctx_for(dims, 0.3, 1234)
     b = O.make_source(dims, 0, 99)
@@ -141,4 +141,36 @@ def test_mixed_absolute_target(cuda):
     with pytest.raises(K.KuQCDError):
         bt.add(ctx, d_b, d_x, sig, solver=K.KQ_SOLVER_MIXED, rel_residual=-1.0, tol=tol)
     bt.close()
+    ctx.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kw", [dict(solver=K.KQ_SOLVER_MIXED, prec=K.KUQCD_HALF),
+                                dict(solver=K.KQ_SOLVER_CGM_WINDOWED), dict(solver=K.KQ_SOLVER_CGM)])
+@pytest.mark.parametrize("stop", ["0.7", "3"])
+def test_pinned_host_buffers_copy_during_the_solve(cuda, monkeypatch, kw, stop):
+    """With page-locked host buffers each solution is copied out as soon as the solver is done with it, while the
+    other shifts still iterate, and copied again if the refinement changes it afterwards (KUQCD_RELAX_STOP=3 stops
+    the multishift above the target, so the mixed solver refines).  The solutions are the pageable path's, bit for
+    bit; the reference-order CGM reports nothing early and copies at the end."""
+    monkeypatch.setenv("KUQCD_RELAX_STOP", stop)
+    dims = (8, 8, 8, 8)
+    ctx, fat, lng = ctx_for(dims, 0.3, 2024)
+    b = O.make_source(dims, 1, 31)
+    sig = list(0.05 ** 2 + np.logspace(-4, 0, 10))
+    tol = (1e-10) ** 2 * float(b @ b)
+    xa, ia = ctx.solve(b, sig, parity=1, tol=tol, rel_residual=1e-10, **kw)
+    xb, ib = ctx.solve(b, sig, parity=1, tol=tol, rel_residual=1e-10, pinned=True, **kw)
+    assert ia.status == 0 and ib.status == 0
+    assert (ia.iter, ia.iter_refine) == (ib.iter, ib.iter_refine)
+    assert ia.copies_during_solve == 0
+    if kw["solver"] == K.KQ_SOLVER_CGM:
+        assert ib.copies_during_solve == 0
+    else:
+        assert ib.copies_during_solve >= len(sig) // 2, ib.copies_during_solve
+    if kw["solver"] == K.KQ_SOLVER_MIXED and stop == "3":
+        assert ib.iter_refine > 0
+    for k, s in enumerate(sig):
+        assert np.array_equal(xa[k], xb[k]), k
+        assert O.true_residual(dims, fat, lng, 1, s, b, xb[k]) <= 1.5e-10, k
     ctx.close()
