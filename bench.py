@@ -170,7 +170,7 @@ def run_ours(args):
     def solver_kw(name):
         if name in ("fp64", "fp64w"):
             # plain CGM stopping rule tol = (rel * |b|)^2 on the recursive residual of every shift; "fp64" keeps the
-            # reference's kernel order, "fp64w" defers the shift updates over windows of 8 iterations
+            # reference's kernel order, "fp64w" defers the shift updates over windows of 16 iterations
             return dict(parity=0, solver=K.KQ_SOLVER_CGM if name == "fp64" else K.KQ_SOLVER_CGM_WINDOWED,
                         prec=K.KUQCD_DOUBLE, max_iter=100000, tol=(REL_RES ** 2) * bnorm2, shift_mode=1)
         return dict(parity=0, solver=K.KQ_SOLVER_MIXED, prec=sloppy[name], max_iter=100000, rel_residual=REL_RES,

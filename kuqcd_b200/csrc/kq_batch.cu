@@ -38,7 +38,7 @@ struct SysDesc {
     int pv, parity, ntiles, pad;
     LinkSet fat[3], lng[3];
     const void *b;
-    void *x, *p0, *s, *tmp, *ring, *pw;
+    void *x, *p0, *tmp, *ring, *pw;
     size_t vb;
     double *partials;  // one per tile
     MsState *st;
@@ -118,7 +118,8 @@ __global__ void __launch_bounds__(BS) bk_init_kernel(const SysDesc *__restrict__
                 st->maxTerm = st->ns;
                 st->wmax = st->ns;
                 st->iter = st->wpos = st->nupd = st->halt = 0;
-                st->mode = 0;
+                st->mode = st->next_mode = 0;
+                st->pp = tot;  // p0 = b
                 // b = 0: x = 0 is the solution; a non-finite source is a breakdown
                 const bool finite = isfinite(tot);
                 st->status = finite ? 0 : KQ_STATUS_BREAKDOWN;
@@ -131,7 +132,8 @@ __global__ void __launch_bounds__(BS) bk_init_kernel(const SysDesc *__restrict__
     }
 }
 
-// K1: tmp = D p0 for the systems whose operator precision is M (one launch per precision, so that each launch is
+// K1: tmp = D p0 and |tmp|^2 -> beta step with <p0, A p0> = sigma0 |p0|^2 + |tmp|^2 (|p0|^2 from the alpha step's
+// recurrence), for the systems whose operator precision is M (one launch per precision, so that each launch is
 // specialised; systems in the other precisions skip their items).  FP64 and HALF get up to 128 registers: at the
 // 85-register cap of three 256-thread CTAs per SM the long-link row rebuild and the HALF decode spill.
 template <int BS, int M>
@@ -139,21 +141,38 @@ __global__ void __launch_bounds__(BS, (M == 1 ? 768 : 512) / BS) bk_dslash1_kern
                                                         const int2 *__restrict__ items, int nitems)
 {
     typedef typename Acc2<M, M>::T T;
+    __shared__ double sm[32];
 #pragma unroll 1
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const int2 w = items[it];
         const SysDesc &d = c_sys[w.x];
-        const MsState *st = d.st;
+        MsState *st = d.st;
         if (!st->active || st->mode != M) continue;
         const int i = w.y * BS + threadIdx.x;
-        if (i >= d.g.vh) continue;
-        T acc[6];
-        dslash_site_t<M, 0, T>(d.g, d.pv, d.fat[M], d.lng[M], d.p0, 1 - d.parity, i, acc);
-        st_spinor_as<M>(d.tmp, d.pv, i, acc);
+        double tt = 0.0;
+        if (i < d.g.vh) {
+            T acc[6];
+            dslash_site_t<M, 0, T>(d.g, d.pv, d.fat[M], d.lng[M], d.p0, 1 - d.parity, i, acc);
+            st_spinor_as<M>(d.tmp, d.pv, i, acc);
+#pragma unroll
+            for (int k = 0; k < 6; ++k) tt += (double)acc[k] * (double)acc[k];
+        }
+        tt = block_sum(tt, sm);
+        if (threadIdx.x == 0) d.partials[w.y] = tt;
+        if (tile_ticket_last(&st->ticket[1], d.ntiles)) {
+            const double tot = tile_partials_sum(d.partials, d.ntiles, sm);
+            if (threadIdx.x < 32) {
+                ms_step_beta(st, st->shift[0] * st->pp + __shfl_sync(0xffffffffu, tot, 0));
+                if (threadIdx.x == 0) st->ticket[1] = 0;
+            }
+        }
+        __syncthreads();
     }
 }
 
-// K2: s = sigma0 p0 - D tmp (FP64), <p0, s> -> beta step, for the systems in precision M
+// K2: r^(i+1) = r^(i) + B0 (sigma0 p0 - D tmp) into the ring (s stays in registers), |r|^2 -> alpha step, for the
+// systems in precision M.  The alpha step picks the next iteration's precision in next_mode, applied in K3, so the
+// K2 launches of the other precisions in this iteration do not pick the system up again.
 template <int BS, int M>
 __global__ void __launch_bounds__(BS, (M == 1 ? 768 : 512) / BS) bk_dslash2_kernel(const SysDesc *__restrict__ sys,
                                                         const int2 *__restrict__ items, int nitems)
@@ -166,59 +185,21 @@ __global__ void __launch_bounds__(BS, (M == 1 ? 768 : 512) / BS) bk_dslash2_kern
         const SysDesc &d = c_sys[w.x];
         MsState *st = d.st;
         if (!st->active || st->mode != M) continue;
-        const int i = w.y * BS + threadIdx.x;
-        double dot = 0.0;
-        if (i < d.g.vh) {
-            T acc[6];
-            dslash_site_t<M, M, T>(d.g, d.pv, d.fat[M], d.lng[M], d.tmp, d.parity, i, acc);
-            double pv6[6], sv[6];
-            ld_spinor<0>(d.p0, d.pv, i, pv6);
-            const double sig = st->shift[0];
-#pragma unroll
-            for (int k = 0; k < 6; ++k) {
-                sv[k] = sig * pv6[k] - (double)acc[k];
-                dot += pv6[k] * sv[k];
-            }
-            st_spinor<0>(d.s, d.pv, i, sv);
-        }
-        dot = block_sum(dot, sm);
-        if (threadIdx.x == 0) d.partials[w.y] = dot;
-        if (tile_ticket_last(&st->ticket[1], d.ntiles)) {
-            const double tot = tile_partials_sum(d.partials, d.ntiles, sm);
-            if (threadIdx.x < 32) {
-                ms_step_beta(st, __shfl_sync(0xffffffffu, tot, 0));
-                if (threadIdx.x == 0) st->ticket[1] = 0;
-            }
-        }
-        __syncthreads();
-    }
-}
-
-// K3: r^(i) = r^(i-1) + B0 s into the ring, |r|^2 -> alpha step (and the next operator precision)
-template <int BS>
-__global__ void __launch_bounds__(BS) bk_r_kernel(const SysDesc *__restrict__ sys, const int2 *__restrict__ items,
-                                                  int nitems)
-{
-    __shared__ double sm[32];
-#pragma unroll 1
-    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-        const int2 w = items[it];
-        const SysDesc &d = c_sys[w.x];
-        MsState *st = d.st;
-        if (!st->active) continue;
         const int itc = st->iter;
         const char *rin = static_cast<const char *>(d.ring) + (size_t)(itc % kWin) * d.vb;
         char *rout = static_cast<char *>(d.ring) + (size_t)((itc + 1) % kWin) * d.vb;
         const int i = w.y * BS + threadIdx.x;
         double nn = 0.0;
         if (i < d.g.vh) {
-            double rv[6], sv[6];
+            T acc[6];
+            dslash_site_t<M, M, T>(d.g, d.pv, d.fat[M], d.lng[M], d.tmp, d.parity, i, acc);
+            double pv6[6], rv[6];
+            ld_spinor<0>(d.p0, d.pv, i, pv6);
             ld_spinor<0>(rin, d.pv, i, rv);
-            ld_spinor<0>(d.s, d.pv, i, sv);
-            const double b0 = st->B[0];
+            const double sig = st->shift[0], b0 = st->B[0];
 #pragma unroll
             for (int k = 0; k < 6; ++k) {
-                rv[k] += b0 * sv[k];
+                rv[k] += b0 * (sig * pv6[k] - (double)acc[k]);
                 nn += rv[k] * rv[k];
             }
             st_spinor<0>(rout, d.pv, i, rv);
@@ -236,7 +217,8 @@ __global__ void __launch_bounds__(BS) bk_r_kernel(const SysDesc *__restrict__ sy
     }
 }
 
-// K4: p0 = r^(i) + a0 p0.  A system that stopped in K3 no longer needs p0.
+// K3: p0 = r^(i) + a0 p0; the next iteration's precision takes effect.  A system that stopped in K2 no longer
+// needs p0.
 template <int BS>
 __global__ void __launch_bounds__(BS) bk_p0_kernel(const SysDesc *__restrict__ sys, const int2 *__restrict__ items,
                                                    int nitems)
@@ -245,22 +227,28 @@ __global__ void __launch_bounds__(BS) bk_p0_kernel(const SysDesc *__restrict__ s
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const int2 w = items[it];
         const SysDesc &d = c_sys[w.x];
-        const MsState *st = d.st;
+        MsState *st = d.st;
         if (!st->active) continue;
         const int i = w.y * BS + threadIdx.x;
-        if (i >= d.g.vh) continue;
-        const char *r = static_cast<const char *>(d.ring) + (size_t)(st->iter % kWin) * d.vb;
-        double rv[6], pv6[6];
-        ld_spinor<0>(r, d.pv, i, rv);
-        ld_spinor<0>(d.p0, d.pv, i, pv6);
-        const double a0 = st->a[0];
+        if (i < d.g.vh) {
+            const char *r = static_cast<const char *>(d.ring) + (size_t)(st->iter % kWin) * d.vb;
+            double rv[6], pv6[6];
+            ld_spinor<0>(r, d.pv, i, rv);
+            ld_spinor<0>(d.p0, d.pv, i, pv6);
+            const double a0 = st->a[0];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) pv6[k] = rv[k] + a0 * pv6[k];
-        st_spinor<0>(d.p0, d.pv, i, pv6);
+            for (int k = 0; k < 6; ++k) pv6[k] = rv[k] + a0 * pv6[k];
+            st_spinor<0>(d.p0, d.pv, i, pv6);
+        }
+        if (tile_ticket_last(&st->ticket[3], d.ntiles) && threadIdx.x == 0) {
+            st->mode = st->next_mode;
+            st->ticket[3] = 0;
+        }
+        __syncthreads();
     }
 }
 
-// K5: windowed shift update of every system that iterated in this window
+// K4: windowed shift update of every system that iterated in this window
 template <int BS>
 __global__ void __launch_bounds__(BS) bk_window_kernel(const SysDesc *__restrict__ sys,
                                                        const int2 *__restrict__ items, int nitems)
@@ -315,7 +303,6 @@ static void enqueue_batch_chunk(const SysDesc *d, const int2 *items, int nitems,
         bk_dslash2_kernel<BS, 0><<<grid, BS, 0, s>>>(d, items, nitems);
         bk_dslash2_kernel<BS, 1><<<grid, BS, 0, s>>>(d, items, nitems);
         bk_dslash2_kernel<BS, 2><<<grid, BS, 0, s>>>(d, items, nitems);
-        bk_r_kernel<BS><<<grid, BS, 0, s>>>(d, items, nitems);
         bk_p0_kernel<BS><<<grid, BS, 0, s>>>(d, items, nitems);
     }
     bk_window_kernel<BS><<<grid, BS, 0, s>>>(d, items, nitems);
@@ -470,7 +457,6 @@ cudaError_t batch_plan(kq_batch *b, int bs, BatchPlan &plan, bool carve_only, si
         d.b = S.d_b;
         d.x = S.d_x;
         d.p0 = c.take(vb);
-        d.s = c.take(vb);
         d.tmp = c.take(vb);
         d.ring = c.take(vb * kWin);
         d.pw = c.take(vb * ns);
@@ -590,7 +576,7 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
             err = cudaGraphLaunch(exec, s);
             if (err != cudaSuccess) break;
             ++chunks;
-            *launches += 8 * kChunk + 1;  // two dslash steps x three precisions + r + p0 per iteration, + window
+            *launches += 7 * kChunk + 1;  // two dslash steps x three precisions + p0 per iteration, + window
             if (chunks > 1000000) break;
         }
         cudaEventRecord(e1, s);

@@ -120,6 +120,8 @@ __device__ __forceinline__ void ms_step_alpha(MsState *st, double lambda2)
         st->lambda2 = lambda2;
         st->a[0] = a0;
         st->rNorm2 = lambda2;
+        // |p_new|^2 = |r_new|^2 + a0^2 |p|^2, since the step makes r_new orthogonal to p
+        st->pp = lambda2 + a0 * a0 * st->pp;
         st->maxTerm = mt;
         st->iter += 1;
         st->wpos = jw + 1;
@@ -130,9 +132,10 @@ __device__ __forceinline__ void ms_step_alpha(MsState *st, double lambda2)
         }
         st->active = (mt > 0 && st->iter < st->max_iter && !halt0 && finite) ? 1 : 0;
         if (!st->active && st->running) atomicSub(st->running, 1);
-        // relaxed operator precision for the next iteration, from the base residual
+        // relaxed operator precision for the next iteration, from the base residual (the batched solver's)
         const double rel2 = lambda2 / st->bnorm2;
-        st->mode = (st->rho16_2 > 0.0 && rel2 < st->rho16_2) ? 2 : (st->rho32_2 > 0.0 && rel2 < st->rho32_2) ? 1 : 0;
+        st->next_mode =
+            (st->rho16_2 > 0.0 && rel2 < st->rho16_2) ? 2 : (st->rho32_2 > 0.0 && rel2 < st->rho32_2) ? 1 : 0;
     }
 }
 

@@ -24,7 +24,8 @@
 //    the residual update uses the operator actually applied, so the recurrence stays exact.
 //
 // Kernels per iteration: K1 tmp = D p0, |tmp|^2 (beta step + x coefficients);  K2 r <- r + B0 (sigma0 p0 - D tmp)
-// into the ring, |r|^2 (alpha step + p coefficients + shift dropping);  K3 p0 <- r + a0 p0, |p0|^2.
+// into the ring, |r|^2 (alpha step + p coefficients + shift dropping + |p0|^2 = |r|^2 + a0^2 |p0|^2, r being
+// orthogonal to the old p0);  K3 p0 <- r + a0 p0.
 // One CUDA graph per operator precision, kChunk iterations each followed by K4, the windowed shift update, which
 // applies the window once it is full (W = 2 kChunk iterations) or the solve has stopped, and otherwise returns at
 // once.  The window sets the shift-update traffic, the chunk the granularity of the precision switches.
@@ -89,7 +90,7 @@ __global__ void __launch_bounds__(kBSm) ms_init_kernel(int vh, int pv, const voi
 }
 
 // K1: tmp = D p0 (p0 FP64; links LP; tmp stored in SO); |tmp|^2, then the beta step with
-// <p0, A p0> = sigma0 |p0|^2 + |tmp|^2
+// <p0, A p0> = sigma0 |p0|^2 + |tmp|^2 (|p0|^2 from the alpha step's recurrence)
 template <int LP, int SO>
 __global__ void __launch_bounds__(kBSm) ms_dslash1_kernel(Geom g, int pv, LinkSet fat, LinkSet lng,
                                                           const void *__restrict__ p0, void *__restrict__ tmp, int q,
@@ -145,29 +146,21 @@ __global__ void __launch_bounds__(kBSm) ms_dslash2_kernel(Geom g, int pv, LinkSe
     if (grid_sum_last_warp(nn, partials, &st->ticket[2], sm, &tot)) ms_step_alpha(st, tot);
 }
 
-// K3: p0 = r^(i) + a0 p0 ; |p0|^2 for the next beta step
+// K3: p0 = r^(i) + a0 p0
 __global__ void __launch_bounds__(kBSm) ms_p0_kernel(int vh, int pv, const char *ring, size_t vb, void *p0,
-                                                     MsState *st, double *partials)
+                                                     const MsState *st)
 {
     if (st->active == 0) return;
-    __shared__ double sm[32];
     const int i = blockIdx.x * kBSm + threadIdx.x;
-    double pp = 0.0;
-    if (i < vh) {
-        const char *r = ring + (size_t)(st->iter % kWin) * vb;
-        double rv[6], pv6[6];
-        ld_spinor<0>(r, pv, i, rv);
-        ld_spinor<0>(p0, pv, i, pv6);
-        const double a0 = st->a[0];
+    if (i >= vh) return;
+    const char *r = ring + (size_t)(st->iter % kWin) * vb;
+    double rv[6], pv6[6];
+    ld_spinor<0>(r, pv, i, rv);
+    ld_spinor<0>(p0, pv, i, pv6);
+    const double a0 = st->a[0];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            pv6[k] = rv[k] + a0 * pv6[k];
-            pp += pv6[k] * pv6[k];
-        }
-        st_spinor<0>(p0, pv, i, pv6);
-    }
-    double tot;
-    if (grid_sum_last(pp, partials, &st->ticket[3], sm, &tot)) st->pp = tot;
+    for (int k = 0; k < 6; ++k) pv6[k] = rv[k] + a0 * pv6[k];
+    st_spinor<0>(p0, pv, i, pv6);
 }
 
 // K4: windowed shift update p_k <- c_k p_k + sum_l d_kl r_l ; x_k <- x_k + e_k p_k + sum_l f_kl r_l
@@ -220,7 +213,7 @@ static void enqueue_ms_chunk(const Geom &g, const GaugeDev &gd, const MsBuffers 
                                                       w.partials);
         ms_dslash2_kernel<LP, SO><<<nb, kBSm, 0, s>>>(g, pv, gd.fat[LP], gd.lng[LP], w.tmp, w.p0, (char *)w.ring,
                                                       w.vb, parity, w.st, w.partials);
-        ms_p0_kernel<<<nb, kBSm, 0, s>>>(g.vh, pv, (const char *)w.ring, w.vb, w.p0, w.st, w.partials);
+        ms_p0_kernel<<<nb, kBSm, 0, s>>>(g.vh, pv, (const char *)w.ring, w.vb, w.p0, w.st);
     }
     ms_window_kernel<<<nb, kBSm, 0, s>>>(g.vh, pv, (const char *)w.ring, w.vb, (char *)w.pw, (char *)w.x, w.st);
 }

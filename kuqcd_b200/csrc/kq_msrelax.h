@@ -15,12 +15,12 @@ struct MsState {
     unsigned ticket[4];
     double tol;
     double Bm1, pAp, lambda2;
-    double pp;  // |p0|^2 (single-system solver: the beta step takes <p0, A p0> = sigma0 |p0|^2 + |D p0|^2)
+    double pp;  // |p0|^2, kept by the recurrence |p'|^2 = |r'|^2 + a0^2 |p|^2; <p0, A p0> = sigma0 |p0|^2 + |D p0|^2
     double shift[kMaxShift];  // reference semantics: shift[0] absolute, shift[j] = sigma_j - sigma_0
     double a[kMaxShift], B[kMaxShift], Z[kMaxShift], Zm1[kMaxShift];
     double c[kMaxShift], e[kMaxShift];           // p_k, x_k coefficients of p_k at the window start
     double d[kMaxShift][kWin], f[kMaxShift][kWin];  // coefficients of the ring residuals
-    int mode, pad3;           // operator precision of the next iteration (0 FP64, 1 FP32, 2 HALF; set on the device)
+    int mode, next_mode;  // batched solver: operator precision of this / the next iteration (0 FP64, 1 FP32, 2 HALF)
     double rho32_2, rho16_2;  // squared relative-residual switch points (0: never)
     int *running;             // batched solver: systems still iterating (decremented when this one stops)
 };
