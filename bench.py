@@ -398,6 +398,26 @@ def ref_cpu_time_per_iter(dims, sample_iters, seed=1000):
     return per_iter
 
 
+def ref_cpu_dslash_seconds(dims, reps=10, seed=1000):
+    """Seconds per FP64 DiracHISQ::Dslash of the reference (oracle/_ref, all host cores) on the bench's fields: a call
+    applying it 1 + reps times minus a call applying it once (field set-up and neighbour tables cancel)."""
+    from oracle import oracle as O
+
+    key = (tuple(dims), seed)
+    if key not in _REF_FIELDS:
+        fat, lng = O.make_links(dims, EPS, seed)
+        _REF_FIELDS.clear()
+        _REF_FIELDS[key] = (fat, lng, O.make_source(dims, 0, seed))
+    fat, lng, b = _REF_FIELDS[key]
+    t = []
+    with quiet_stdout():
+        for n in (1, 1 + reps):
+            t0 = time.perf_counter()
+            O.ref_dslash(dims, fat, lng, b, 1, reps=n)
+            t.append(time.perf_counter() - t0)
+    return max(t[1] - t[0], 0.0) / reps or t[1] / (1 + reps)
+
+
 def cpu_baseline_sample(args, iters_hint=None):
     from oracle import oracle as O
 
@@ -408,10 +428,14 @@ def cpu_baseline_sample(args, iters_hint=None):
     t_it = ref_cpu_time_per_iter(dims, sample)
     iters = ref_iterations_needed() or iters_hint or 0
     solve_s = t_it * iters if iters else None
+    t_d = ref_cpu_dslash_seconds(dims)
+    vh = int(np.prod(dims)) // 2
     return {"value": (1.0 / solve_s) if solve_s else None, "unit": "solves/s", "cores": os.cpu_count(),
             "kind": "reference", "seconds_per_iteration": t_it,
+            "dslash_ms": t_d * 1e3, "dslash_gbs": 2400.0 * vh / t_d / 1e9,
             "sample": f"{sample} CGM iterations of the reference on the same workload, extrapolated to "
-                      f"{iters} iterations (its iteration count to convergence)"}
+                      f"{iters} iterations (its iteration count to convergence); FP64 dslash: mean of 10 "
+                      f"applications (compulsory 2400 B per output site)"}
 
 
 def run_reference(args):

@@ -126,10 +126,11 @@ def true_residual(dims, fat, lng, parity, sigma, b, x):
 
 
 # ---------------------------------------------------------------- reference library
-def ref_dslash(dims, fat, lng, src, dst_parity):
+def ref_dslash(dims, fat, lng, src, dst_parity, reps=1):
+    """The reference's DiracHISQ::Dslash (one set-up of fields and neighbour tables, then `reps` applications)."""
     out = np.zeros_like(src)
     f = ref().kqref_dslash_d if src.dtype == np.float64 else ref().kqref_dslash_f
-    st = f((C.c_uint * 4)(*dims), _p(fat), _p(lng), _p(src), _p(out), dst_parity, 1)
+    st = f((C.c_uint * 4)(*dims), _p(fat), _p(lng), _p(src), _p(out), dst_parity, reps)
     assert st == 0
     return out
 

@@ -122,3 +122,17 @@ def test_port_cgm_float_close_to_double():
                   1e-10 * float(b @ b), 2000)
     for k in range(2):
         assert np.abs(xf[k] - xd[k]).max() < 1e-4 * np.abs(xd[k]).max()
+
+
+@needs_ref
+def test_reference_dslash_repetitions_and_bench_cpu_timing():
+    """Applying the reference dslash several times in one call gives the single application's result (the CPU
+    baseline times 11 applications against 1, so that field set-up cancels), and the bench helper returns a
+    positive per-application time."""
+    import bench
+
+    dims = (4, 4, 4, 8)
+    fat, lng = O.make_links(dims, 0.3, 5)
+    src = O.make_source(dims, 0, 6)
+    assert np.array_equal(O.ref_dslash(dims, fat, lng, src, 1, reps=3), O.ref_dslash(dims, fat, lng, src, 1))
+    assert bench.ref_cpu_dslash_seconds(dims) > 0.0
