@@ -456,13 +456,17 @@ def run_reference(args):
     iters = ref_iterations_needed()
     solve_s = t_it * iters
     v = 1.0 / solve_s
+    t_d = ref_cpu_dslash_seconds(dims)
     res = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": solve_s * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
         "config": {"workload": workload_name(dims), "solver": "reference CGM (CPU)"},
         "cpu_baseline": {"value": v, "unit": "solves/s", "cores": os.cpu_count(), "kind": "reference",
-                         "sample": f"{sample} CGM iterations per step, extrapolated to {iters} iterations"},
+                         "seconds_per_iteration": t_it, "dslash_ms": t_d * 1e3,
+                         "dslash_gbs": 2400.0 * (int(np.prod(dims)) // 2) / t_d / 1e9,
+                         "sample": f"{sample} CGM iterations per step, extrapolated to {iters} iterations; FP64 "
+                                   f"dslash: mean of 10 applications"},
         "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(res))
