@@ -101,8 +101,9 @@ def test_dslash_is_anti_hermitian_between_parities():
 @pytest.mark.parametrize("dims,parity,nshift", [((8, 8, 8, 8), 0, 12), ((6, 4, 4, 6), 1, 12), ((4, 4, 4, 8), 0, 16)])
 def test_gpu_recurrences_match_reference_order(dims, parity, nshift):
     """Iteration counts agree to one.  (On a lattice as small as 4^4, where the solve takes about a third as many
-    iterations as the system has unknowns, rounding alone moves the stop by a few iterations: the windowed form with either
-    step-length formula stops at 282 there against the reference order's 287, solutions equal to 6e-12.)"""
+    iterations as the system has unknowns, rounding alone moves the stop by a few iterations: the windowed form
+    with either step-length formula stops at 282 there against the reference order's 287, solutions equal to
+    6e-12.)"""
     fat, lng = O.make_links(dims, 0.3, 40 + nshift)
     b = O.make_source(dims, parity, 7)
     m, sig = 0.05, np.logspace(-4, 0, nshift)
