@@ -63,8 +63,8 @@ EXPORTED_SYMBOLS = [
     "kq_kuqcd_init", "kq_kuqcd_load_gaugefield", "kq_kuqcd_solve_multishift", "kq_kuqcd_gauge_free",
     "kq_kuqcd_end", "kq_context_create", "kq_context_destroy", "kq_load_links", "kq_prepare_links",
     "kq_spinor_bytes", "kq_spinor_upload", "kq_spinor_download", "kq_spinor_convert", "kq_dslash", "kq_mdagm",
-    "kq_mdagm_noalloc", "kq_dslash_full", "kq_mdagm_full", "kq_long_links_compressed", "kq_slab_set", "kq_slab_face_bytes",
-    "kq_slab_pack_faces", "kq_slab_link_face_bytes", "kq_slab_pack_link_face", "kq_slab_set_link_ghosts",
+    "kq_mdagm_noalloc", "kq_dslash_full", "kq_mdagm_full", "kq_long_links_compressed", "kq_slab_set",
+    "kq_slab_face_bytes", "kq_slab_pack_faces", "kq_slab_link_face_bytes", "kq_slab_pack_link_face", "kq_slab_set_link_ghosts",
     "kq_slab_dslash", "kq_field_axpby", "kq_field_dot",
     "kq_solve_multishift", "kq_solve_multishift_device", "kq_true_residuals", "kq_make_links_record",
     "kq_make_source_record", "kq_last_error", "kq_batch_create", "kq_batch_destroy", "kq_batch_add",
