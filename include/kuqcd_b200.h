@@ -76,12 +76,12 @@ KuQCDStatus kq_dslash(kq_context *ctx, int prec, const void *d_src, void *d_dst,
 KuQCDStatus kq_mdagm(kq_context *ctx, int prec, double sigma, const void *d_src, void *d_dst, void *d_tmp,
                      int parity, void *stream);
 /* kq_mdagm without a caller temporary and without any device allocation (no counterpart in the reference).
- * For callers that cannot allocate while they apply the operator: work being recorded into a CUDA graph, where
- * cudaMalloc is not allowed during capture, or applications whose own pool owns nearly all device memory.  The
- * temporary comes from a 32 MiB array that each GPU loading the library holds until exit; larger fields are
- * rejected with KUQCD_ERR_INVALID_PARAM.  All calls share that array: calls overlapping on the GPU race.  Links
- * must already be resident in prec.  The first call on a device looks up the array's address; make it before any
- * stream capture. */
+ * For callers that cannot let the library allocate while they apply the operator: applications whose own memory
+ * pool reserves nearly all of HBM, and latency-critical loops where cudaMalloc / cudaFree may synchronise the
+ * device.  The temporary comes from a 32 MiB array that each GPU loading the library holds until exit; larger
+ * fields are rejected with KUQCD_ERR_INVALID_PARAM.  All calls share that array: calls overlapping on the GPU race.
+ * Links must already be resident in prec.  The first call on a device looks up the array's address; make it before
+ * any stream capture, and do not use this entry point on a device after a cudaDeviceReset in the same process. */
 KuQCDStatus kq_mdagm_noalloc(kq_context *ctx, int prec, double sigma, const void *d_src, void *d_dst, int parity,
                              void *stream);
 
@@ -231,6 +231,10 @@ KuQCDStatus kq_net_train_pair(kq_net *net, const void *d_r, const void *d_e, int
                               double *loss);
 /* Adam step on the accumulated gradient times grad_scale; clears the accumulator */
 KuQCDStatus kq_net_adam(kq_net *net, float lr, float grad_scale);
+/* Test hook (no reference counterpart): sets the device word that a tensor-core tile sets when its bounded wait runs
+ * out, so that the next kq_net_apply / kq_net_train_pair reports KUQCD_ERR_UNKNOWN_ERROR once and the call after it
+ * succeeds.  Exercises the error path without making any GPU wait time out. */
+KuQCDStatus kq_net_raise_fault_for_test(kq_net *net);
 /* Polish every shift of d_x (initial guesses, num_shift FP64 fields) to the FP64 true relative residual
  * param->rel_residual with FCG preconditioned by net (NULL: plain CG, also the fallback on breakdown, stagnation
  * or an exhausted budget).  info->iter_refine: all polish iterations; info->iter: those that applied the net. */

@@ -339,6 +339,14 @@ KQ_API KuQCDStatus kq_net_train_pair(kq_net *n, const void *d_r, const void *d_e
     return status_of(e);
 }
 
+// sets the device fault word the network's tensor-core tiles raise on a timed-out wait, from the host
+KQ_API KuQCDStatus kq_net_raise_fault_for_test(kq_net *n)
+{
+    if (!n) return KUQCD_ERR_NULL_POINTER;
+    cudaSetDevice(n->ctx->device);
+    return status_of(ptc_raise_fault_for_test());
+}
+
 // Adam step with the accumulated gradient scaled by grad_scale (e.g. 1/batch); clears the accumulator
 KQ_API KuQCDStatus kq_net_adam(kq_net *n, float lr, float grad_scale)
 {
@@ -346,16 +354,8 @@ KQ_API KuQCDStatus kq_net_adam(kq_net *n, float lr, float grad_scale)
     cudaSetDevice(n->ctx->device);
     cudaStream_t s = n->ctx->stream;
     n->step += 1;
-    // scale the gradient in place (a few thousand floats), then Adam
-    if (grad_scale != 1.0f) {
-        std::vector<float> h(n->nw);
-        cudaMemcpyAsync(h.data(), n->g, n->nw * 4, cudaMemcpyDeviceToHost, s);
-        cudaStreamSynchronize(s);
-        for (float &x : h) x *= grad_scale;
-        cudaMemcpyAsync(n->g, h.data(), n->nw * 4, cudaMemcpyHostToDevice, s);
-    }
-    cudaError_t e = ptc_adam(n->w, n->g, n->m, n->v, (int)n->nw, lr, n->step, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(n->g, 0, n->nw * 4, s);
+    // the kernel scales the gradient, steps and clears the accumulator
+    cudaError_t e = ptc_adam(n->w, n->g, n->m, n->v, (int)n->nw, lr, grad_scale, n->step, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     n->bt_dirty = true;
     return status_of(e);

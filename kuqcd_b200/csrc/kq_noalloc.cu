@@ -1,10 +1,10 @@
 // kq_mdagm_noalloc: sigma*src - D_pq D_qp src without any device allocation.
 //
-// Who needs it: callers that must not allocate device memory while they run the operator -- code that records its
-// work into a CUDA graph (cudaMalloc/cudaFree are not permitted inside stream capture), and applications that hand
-// nearly all of HBM to their own memory pool and cannot let a library allocate behind their back.  kq_mdagm asks the
-// caller for the parity-(1-p) temporary; this variant takes it from a fixed device array that every GPU loading the
-// library holds from module load until process exit.
+// Who needs it: callers that cannot have the library allocate device memory while they run the operator.  Some
+// applications reserve nearly all of HBM for their own memory pool at start-up, so a cudaMalloc here would fail or
+// fragment their pool; others apply the operator inside a latency-critical loop, where cudaMalloc / cudaFree can
+// synchronise the whole device.  kq_mdagm asks the caller for the parity-(1-p) temporary; this variant takes it from
+// a fixed device array that every GPU loading the library holds from module load until process exit.
 //
 // Limits and sharing:
 //   * the temporary needs kq_spinor_bytes(ctx, prec) bytes; anything above kStaticScratchBytes (32 MiB) is rejected
@@ -15,7 +15,9 @@
 //   * the links must already be resident in `prec` (kq_load_links / kq_prepare_links): this call never converts or
 //     allocates them;
 //   * the first call on a device looks up the array's device address (cudaGetSymbolAddress with that device
-//     current) and caches it; make that first call before any stream capture.
+//     current) and caches it for the life of the process; make that first call before any stream capture.  A
+//     cudaDeviceReset in the same process invalidates the cached address: do not call this entry point on a
+//     device after resetting it.
 #include <mutex>
 
 #include "kq_context.h"

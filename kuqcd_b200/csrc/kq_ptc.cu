@@ -409,12 +409,15 @@ __global__ void ptc_loss_kernel(int vh, int pv, const float2 *__restrict__ y, co
 }
 
 // Adam on the real and imaginary parts of all weights
-__global__ void ptc_adam_kernel(float *w, const float *grad, float *m, float *v, int n, float lr, float b1, float b2,
-                                float eps, int step)
+// Adam on grad * grad_scale (the accumulated gradient of a batch times 1/batch); the accumulator is cleared here, so
+// the next batch starts from zero without a separate memset
+__global__ void ptc_adam_kernel(float *w, float *grad, float *m, float *v, int n, float lr, float grad_scale, float b1,
+                                float b2, float eps, int step)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    const float gk = grad[k];
+    const float gk = grad[k] * grad_scale;
+    grad[k] = 0.0f;
     m[k] = b1 * m[k] + (1 - b1) * gk;
     v[k] = b2 * v[k] + (1 - b2) * gk * gk;
     const float mh = m[k] / (1 - powf(b1, (float)step)), vh = v[k] / (1 - powf(b2, (float)step));
@@ -452,10 +455,21 @@ cudaError_t ptc_check_fault(cudaStream_t s)
     KQ_CUDA_TRY(cudaMemcpyAsync(&h, f, sizeof(int), cudaMemcpyDeviceToHost, s));
     KQ_CUDA_TRY(cudaStreamSynchronize(s));
     if (h) {
+        // the word reports this call's failure once; cleared so that the next call starts clean
+        KQ_CUDA_TRY(cudaMemsetAsync(f, 0, sizeof(int), s));
+        KQ_CUDA_TRY(cudaStreamSynchronize(s));
         set_last_error("ptc: tensor-core tile did not complete within the wait limit");
         return cudaErrorLaunchTimeout;
     }
     return cudaSuccess;
+}
+
+cudaError_t ptc_raise_fault_for_test()
+{
+    int *f = fault_flag();
+    if (!f) return cudaErrorInvalidDevicePointer;
+    const int one = 1;
+    return cudaMemcpy(f, &one, sizeof(int), cudaMemcpyHostToDevice);
 }
 
 template <int CIN, int COUT>
@@ -551,9 +565,10 @@ cudaError_t ptc_loss(const Geom &g, const float2 *y, const void *e, int parity, 
     return cudaSuccess;
 }
 
-cudaError_t ptc_adam(float *w, const float *grad, float *m, float *v, int n, float lr, int step, cudaStream_t s)
+cudaError_t ptc_adam(float *w, float *grad, float *m, float *v, int n, float lr, float grad_scale, int step,
+                     cudaStream_t s)
 {
-    ptc_adam_kernel<<<(n + 255) / 256, 256, 0, s>>>(w, grad, m, v, n, lr, 0.9f, 0.999f, 1e-8f, step);
+    ptc_adam_kernel<<<(n + 255) / 256, 256, 0, s>>>(w, grad, m, v, n, lr, grad_scale, 0.9f, 0.999f, 1e-8f, step);
     return cudaGetLastError();
 }
 

@@ -16,6 +16,8 @@ cudaError_t ptc_wgrad(const Geom &g, const LinkSet &fat, int cin, int cout, cons
 // cudaErrorLaunchTimeout when a forward tile's tensor-core work did not complete within its wait limit (the
 // kernels then leave that tile unwritten); synchronises the stream
 cudaError_t ptc_check_fault(cudaStream_t s);
+// sets the fault word of the current device from the host, as a timed-out tile would (tests of the error path)
+cudaError_t ptc_raise_fault_for_test();
 int ptc_kpad(int cin);
 int ptc_npad(int cout);
 int ptc_tiles(const Geom &g);
@@ -24,6 +26,8 @@ cudaError_t ptc_embed(const Geom &g, const void *src, int parity, float2 *act, d
 cudaError_t ptc_extract(const Geom &g, const float2 *act, int parity, void *dst, double scale, cudaStream_t s);
 cudaError_t ptc_loss(const Geom &g, const float2 *y, const void *e, int parity, double inv_e2, float2 *gout,
                      double *partials, double *loss_host, cudaStream_t s);
-cudaError_t ptc_adam(float *w, const float *grad, float *m, float *v, int n, float lr, int step, cudaStream_t s);
+// Adam step on grad * grad_scale; clears grad
+cudaError_t ptc_adam(float *w, float *grad, float *m, float *v, int n, float lr, float grad_scale, int step,
+                     cudaStream_t s);
 
 }  // namespace kq

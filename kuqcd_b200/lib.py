@@ -70,7 +70,8 @@ EXPORTED_SYMBOLS = [
     "kq_make_source_record", "kq_last_error", "kq_batch_create", "kq_batch_destroy", "kq_batch_add",
     "kq_batch_size", "kq_batch_solve", "kq_batch_system_info", "kq_net_create", "kq_net_destroy",
     "kq_net_num_weights", "kq_net_set_weights", "kq_net_get_weights", "kq_net_get_grad", "kq_net_zero_grad",
-    "kq_net_set_context", "kq_net_apply", "kq_net_train_pair", "kq_net_adam", "kq_fcg_polish",
+    "kq_net_set_context", "kq_net_apply", "kq_net_train_pair", "kq_net_adam", "kq_net_raise_fault_for_test",
+    "kq_fcg_polish",
 ]
 
 
@@ -152,6 +153,7 @@ def library() -> C.CDLL:
         "kq_net_apply": (i, [vp, vp, vp, i]),
         "kq_net_train_pair": (i, [vp, vp, vp, i, d, C.POINTER(d)]),
         "kq_net_adam": (i, [vp, C.c_float, C.c_float]),
+        "kq_net_raise_fault_for_test": (i, [vp]),
         "kq_fcg_polish": (i, [vp, vp, C.POINTER(SolveParam), vp, vp, C.POINTER(SolveInfo)]),
     }
     for name, (res, args) in sig.items():

@@ -64,3 +64,25 @@ def test_failed_allocation_reports_no_memory(cuda):
     big.close()
     ctx, fat, lng = ctx_for()
     still_solves(ctx, fat, lng)
+
+
+@pytest.mark.gpu
+def test_net_fault_is_reported_once(cuda):
+    """A tensor-core tile whose bounded wait ran out sets a device word; the next network call reports it and clears
+    it, so the call after that succeeds.  The word is set from the host here: no wait is made to time out."""
+    import torch
+
+    ctx, fat, lng = ctx_for()
+    net = K.Net(ctx, (1, 8, 8))
+    vb = ctx.spinor_bytes(K.KUQCD_DOUBLE)
+    d_in = torch.zeros(vb, dtype=torch.uint8, device="cuda:0")
+    ctx.upload(K.KUQCD_DOUBLE, O.make_source(DIMS, 0, 9), d_in)
+    d_out = torch.zeros_like(d_in)
+    net.apply(d_in, d_out, 0)
+    assert K.library().kq_net_raise_fault_for_test(net._h) == 0
+    with pytest.raises(K.KuQCDError):
+        net.apply(d_in, d_out, 0)
+    assert b"wait limit" in K.library().kq_last_error()
+    net.apply(d_in, d_out, 0)
+    net.close()
+    still_solves(ctx, fat, lng)

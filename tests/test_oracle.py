@@ -127,12 +127,22 @@ def test_port_cgm_float_close_to_double():
 @needs_ref
 def test_reference_dslash_repetitions_and_bench_cpu_timing():
     """Applying the reference dslash several times in one call gives the single application's result (the CPU
-    baseline times 11 applications against 1, so that field set-up cancels), and the bench helper returns a
-    positive per-application time."""
+    baseline times 11 applications against 1, so that field set-up cancels); the bench's sampled reference solve
+    (calls stopped after 1 and 1 + n iterations) extrapolates to a positive time, and a complete solve through the
+    same loaded gauge field converges to the workload's residual."""
     import bench
 
-    dims = (4, 4, 4, 8)
-    fat, lng = O.make_links(dims, 0.3, 5)
-    src = O.make_source(dims, 0, 6)
-    assert np.array_equal(O.ref_dslash(dims, fat, lng, src, 1, reps=3), O.ref_dslash(dims, fat, lng, src, 1))
-    assert bench.ref_cpu_dslash_seconds(dims) > 0.0
+    cfg = dict(bench.CONFIGS["32"], dims=(4, 4, 4, 8), ref_iters=40)
+    fat, lng = O.make_links(cfg["dims"], cfg["eps"], 5)
+    src = O.make_source(cfg["dims"], 0, 6)
+    assert np.array_equal(O.ref_dslash(cfg["dims"], fat, lng, src, 1, reps=3),
+                          O.ref_dslash(cfg["dims"], fat, lng, src, 1))
+    assert bench.ref_dslash_seconds(cfg, fat, lng, src) > 0.0
+    rs = bench.RefSolver(cfg, fat, lng, src)
+    solve_s, t1, per_iter = bench.ref_sample(rs, cfg, 3)
+    assert solve_s >= t1 > 0.0 and per_iter > 0.0
+    t, it = rs.solve(100000)
+    assert t > 0.0 and 1 < it < 100000
+    res = [O.true_residual(cfg["dims"], fat, lng, 0, s, src, x) for s, x in zip(bench.shifts_abs(cfg), rs.xs)]
+    assert max(res) < 1e-9
+    rs.close()

@@ -1,6 +1,7 @@
-"""kq_mdagm_noalloc: the operator sigma - D_pq D_qp for callers that cannot allocate device memory while they run it
-(work captured into a CUDA graph, applications whose pool owns the device memory).  Its temporary lives in a fixed
-device array of the library, so the results must equal kq_mdagm's with a caller-provided temporary, call after call.
+"""kq_mdagm_noalloc: the operator sigma - D_pq D_qp for callers that cannot let the library allocate device memory
+while they run it (an application whose own pool holds nearly all of HBM, a latency-critical loop where cudaMalloc
+may synchronise the device).  Its temporary lives in a fixed device array of the library, so the results must equal
+kq_mdagm's with a caller-provided temporary, call after call.
 
 This file sorts last so that a run stopping at the first failure has already run every other test."""
 import numpy as np
@@ -16,7 +17,7 @@ def _field(ctx, prec):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("prec,tol", [(K.KUQCD_DOUBLE, 1e-13), (K.KUQCD_SINGLE, 1e-6)])
+@pytest.mark.parametrize("prec,tol", [(K.KUQCD_DOUBLE, 1e-13), (K.KUQCD_SINGLE, 1e-6), (K.KUQCD_HALF, 1e-6)])
 def test_noalloc_matches_kq_mdagm_twice(cuda, prec, tol):
     dims = (8, 8, 8, 8)
     fat, lng = O.make_links(dims, 0.3, 42)
