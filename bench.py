@@ -601,9 +601,11 @@ def run_reference(args):
     return res
 
 
-def run_batch(args):
-    """Batched multi-system workload: 24 independent systems, 8 each on 16^4, 24^3x48 and 32^4, own gauge field
-    (eps ~ U[0.2,0.4]), mass (m ~ U[0.01,0.1]), 8-16 shifts log-spaced 1e-4..1 and Gaussian source, all seeded.
+def run_batch(args, shared=False):
+    """Batched multi-system workload: 24 systems, 8 each on 16^4, 24^3x48 and 32^4, own mass (m ~ U[0.01,0.1]),
+    8-16 shifts log-spaced 1e-4..1 and Gaussian source, all seeded; every system has its own gauge field
+    (eps ~ U[0.2,0.4]) -- or, with shared=True (--config batch-rhs), the 8 systems of each lattice share one gauge
+    field (many sources and masses on one configuration), so the grouped dslash loads each link once for all of them.
     One step = all 24 solved to per-shift true residual 1e-10 by kq_batch_solve (persistent launches over every
     system's tiles, CUDA graphs, autotuned shape); compared with the same 24 solved one after another."""
     import torch
@@ -614,16 +616,21 @@ def run_batch(args):
     rng = np.random.default_rng(4242)
     lattices = [(16, 16, 16, 16)] * 8 + [(24, 24, 24, 48)] * 8 + [(32, 32, 32, 32)] * 8
     systems = []
+    field_ctx = {}
     for i, dims in enumerate(lattices):
         eps, mass, ns = rng.uniform(0.2, 0.4), rng.uniform(0.01, 0.1), int(rng.integers(8, 17))
         V, Vh = int(np.prod(dims)), int(np.prod(dims)) // 2
-        ctx = K.Context(dims)
-        dfat = torch.empty(V * 72, dtype=torch.float64, device="cuda")
-        dlng = torch.empty(V * 72, dtype=torch.float64, device="cuda")
-        ctx.make_links(eps, 5000 + i, dfat, dlng)
-        ctx.load_links(K.KUQCD_FAT_LINK, dfat.cpu().numpy())
-        ctx.load_links(K.KUQCD_LONG_LINK, dlng.cpu().numpy())
-        del dfat, dlng
+        if shared and dims in field_ctx:
+            ctx = field_ctx[dims]
+        else:
+            ctx = K.Context(dims)
+            dfat = torch.empty(V * 72, dtype=torch.float64, device="cuda")
+            dlng = torch.empty(V * 72, dtype=torch.float64, device="cuda")
+            ctx.make_links(eps, 5000 + i, dfat, dlng)
+            ctx.load_links(K.KUQCD_FAT_LINK, dfat.cpu().numpy())
+            ctx.load_links(K.KUQCD_LONG_LINK, dlng.cpu().numpy())
+            del dfat, dlng
+            field_ctx[dims] = ctx
         db = torch.empty(Vh * 6, dtype=torch.float64, device="cuda")
         ctx.make_source(0, 5000 + i, db)
         vb = ctx.spinor_bytes(K.KUQCD_DOUBLE)
@@ -672,16 +679,21 @@ def run_batch(args):
         "warmup": args.warmup, "ms_per_step": t_b * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64+f32" + ("+f16(int16+norm)" if prec == K.KUQCD_HALF else ""),
         "data": "synthetic (seeded on device)",
-        "config": {"workload": "24 systems: 8 x 16^4, 8 x 24^3x48, 8 x 32^4; eps U[0.2,0.4], m U[0.01,0.1], 8-16 "
-                               "shifts 1e-4..1, per-shift true residual 1e-10", "solver": "kq_batch_solve (mixed)",
-                   "tile": info.tile, "ctas_per_sm": info.ctas_per_sm, "max_iterations": info.iterations,
-                   "refined_systems": info.refined_systems, "max_true_residual": bt[-1][2]},
+        "config": {"workload": ("24 systems: 8 x 16^4, 8 x 24^3x48, 8 x 32^4; "
+                                + ("one gauge field per lattice shared by its 8 systems (eps U[0.2,0.4])"
+                                   if shared else "eps U[0.2,0.4], own gauge field each")
+                                + ", m U[0.01,0.1], 8-16 shifts 1e-4..1, per-shift true residual 1e-10"),
+                   "solver": "kq_batch_solve (mixed)", "gauge_fields": len(set(id(c) for c, *_ in systems)),
+                   "tile": info.tile, "ctas_per_sm": info.ctas_per_sm, "rhs_per_cta": info.rhs_per_cta,
+                   "sites_per_thread": info.sites_per_thread, "groups": info.groups,
+                   "max_iterations": info.iterations, "refined_systems": info.refined_systems,
+                   "max_true_residual": bt[-1][2]},
         "sequential": {"ms_per_step": t_s * 1e3, "max_true_residual": st[-1][1], "speedup_of_batched": t_s / t_b},
         "gpu_launches": int(info.kernel_launches), "clocks": clk.summary(),
     }
     print(json.dumps(res))
     bobj.close()
-    for ctx, *_ in systems:
+    for ctx in set(c for c, *_ in systems):
         ctx.close()
     return res
 
@@ -781,7 +793,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--solver", choices=["mixed", "mixed-half", "fp64", "fp64w"], default="mixed-half")
-    ap.add_argument("--config", choices=list(CONFIGS) + ["batch", "learned"], default="48")
+    ap.add_argument("--config", choices=list(CONFIGS) + ["batch", "batch-rhs", "learned"], default="48")
     ap.add_argument("--learned-train", type=int, default=20)
     ap.add_argument("--learned-test", type=int, default=5)
     ap.add_argument("--learned-pairs", type=int, default=2)
@@ -799,12 +811,12 @@ def main():
         else:
             run_learned(args)
         return
-    if args.config == "batch":
+    if args.config in ("batch", "batch-rhs"):
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the batched workload has no reference "
                                                                   "counterpart; run the reference per system"}))
         else:
-            run_batch(args)
+            run_batch(args, shared=args.config == "batch-rhs")
         return
     if args.cpu_sample_iters is None:
         dims = args.dims or CONFIGS[args.config]["dims"]

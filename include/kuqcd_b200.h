@@ -95,6 +95,30 @@ KuQCDStatus kq_dslash_full(kq_context *ctx, int prec, const void *d_src, void *d
 KuQCDStatus kq_mdagm_full(kq_context *ctx, int prec, double sigma, const void *d_src, void *d_dst, void *d_tmp,
                           void *stream);
 
+/* ---------------------------------------------------------------- host-record operators
+ * The class-level API of the reference (DiracHISQ::Dslash / MdaggM, dirac_hisq.cpp:409-462; the BLAS-1 free
+ * functions of spinor_field.h:40-62) keeps field values in host memory (LatticeField::data, lattice_field.h:23-39).
+ * These calls back the header-only classes of include/dirac_hisq.h, spinor_field.h, ...: each copies its operands
+ * to the GPU, runs the kernels there and copies the result back before it returns.  Records are NORMAL_ORDER host
+ * records (layout above; full-lattice records hold the even sites, then the odd sites). */
+/* page-locked host memory for field storage (plain 64-byte aligned memory if page-locking fails) */
+KuQCDStatus kq_host_alloc(size_t bytes, void **out);
+void kq_host_free(void *p);
+enum { KQ_OP_DSLASH = 0, KQ_OP_DD = 1, KQ_OP_SIGMA_MINUS_DD = 2 };
+/* h_dst (parity `parity`, or KQ_PARITY_FULL) = op(h_src):
+ *   KQ_OP_DSLASH          D h_src, h_src on the other parity (DiracHISQ::Dslash, dirac_hisq.cpp:409-455)
+ *   KQ_OP_DD              D D h_src, h_src on the same parity (DiracHISQ::MdaggM, dirac_hisq.cpp:457-462)
+ *   KQ_OP_SIGMA_MINUS_DD  sigma h_src - D D h_src (MdaggM followed by Axmy, inverter_cgm.cpp:45-46)
+ * prec: precision of the operator (links prepared on first use); host_prec: DOUBLE or SINGLE records. */
+KuQCDStatus kq_apply_host(kq_context *ctx, int op, int prec, double sigma, const void *h_src, void *h_dst,
+                          int parity, int host_prec);
+/* h_y = a h_x + b h_y over n reals of host_prec, computed in host_prec.  Covers Axmy, Axpy, Ymax, Axpby and the
+ * field operators of spinor_field.cpp:62-200. */
+KuQCDStatus kq_vec_axpby(int device, int host_prec, size_t n, double a, const void *h_x, double b, void *h_y);
+/* *out = sum_i h_x[i] h_y[i] over n reals, accumulated in FP64 in a fixed order (RealDot / Norm2,
+ * spinor_field.cpp:200-252; h_x == h_y gives Norm2) */
+KuQCDStatus kq_vec_dot(int device, int host_prec, size_t n, const void *h_x, const void *h_y, double *out);
+
 /* ---------------------------------------------------------------- domain decomposition along t
  * The multi-rank path of the reference's dslash (halo pack / exchange, dirac_hisq.cpp:236-407; Communicator,
  * communication.cpp:73-138) for one GPU per rank.  Each rank's context holds its slab of the global lattice
@@ -182,8 +206,10 @@ KuQCDStatus kq_true_residuals(kq_context *ctx, int parity, int num_shift, const 
 
 /* ---------------------------------------------------------------- batched systems
  * Many independent systems (each its own context: lattice, links; its own shifts and source) solved together: each
- * kernel of an iteration is one persistent launch over all systems' site tiles, captured in CUDA graphs; launch
- * shape autotuned and cached on disk (KUQCD_TUNE_CACHE).  No reference counterpart: the reference solves one
+ * kernel of an iteration is one persistent launch over all systems' site tiles, captured in CUDA graphs.  Systems
+ * added with the same context (several sources or masses on one gauge field) and parity are grouped: the dslash
+ * loads each link once for every member of the group (multi-RHS).  Launch shape -- threads per CTA, CTAs per SM,
+ * right-hand sides per CTA, sites per thread -- autotuned on the batch and cached on disk (KUQCD_TUNE_CACHE).  No reference counterpart: the reference solves one
  * system per kuqcd_solve_multishift call (kuqcd.cpp:404-445), so this replaces a loop of such calls. */
 typedef struct kq_batch kq_batch;
 typedef struct {
@@ -196,6 +222,9 @@ typedef struct {
     double max_true_residual; /* over the KQ_SOLVER_MIXED systems' shifts (FP64, after any refinement) */
     int refined_systems;      /* systems the FP64 check sent to refinement */
     int tuned_now;            /* 1 when this call measured the launch shape */
+    int rhs_per_cta;          /* systems on one gauge field whose dslash shares each link load (1, 2, 4 or 8) */
+    int sites_per_thread;     /* sites each thread handles per work item */
+    int groups;               /* groups of systems sharing link loads (+ systems solved on their own) */
 } kq_batch_info;
 
 KuQCDStatus kq_batch_create(int device, kq_batch **out);

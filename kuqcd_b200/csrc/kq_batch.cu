@@ -17,6 +17,7 @@
 // window of the actual batch (kq_tune.cu), cached on disk.  Systems large enough to fill the GPU alone go through
 // the single-system solver instead, concurrently with the batched small ones (kq_batch_solve).
 #include <algorithm>
+#include <cstdio>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -44,12 +45,23 @@ struct SysDesc {
     MsState *st;
 };
 
-// The descriptors live in constant memory: every CTA works on one system at a time, so the (warp-uniform) indexed
-// constant loads are cheap and the fields need not be held in registers across the dslash (with the descriptors in
-// global memory the FP64 kernels needed ~40 more registers and lost occupancy).  One batch solves at a time per
-// process (kq_batch_solve holds a lock); at most kMaxBatch systems.
+// Systems that share one gauge field (the same context) and parity form a group of up to R members; the dslash
+// kernels work on (group, tile) items and load every link once for all members of the group that run in the
+// kernel's operator precision (the multi-RHS form of the dslash).  A group's p0 and tmp fields are consecutive,
+// vb bytes apart, so member r's field is the group base + r * vb.
+constexpr int kMaxR = 8;
+struct GroupDesc {
+    int n;             // members
+    int mem[kMaxR];    // system index of member r
+};
+
+// The descriptors live in constant memory: every CTA works on one system (or group) at a time, so the
+// (warp-uniform) indexed constant loads are cheap and the fields need not be held in registers across the dslash
+// (with the descriptors in global memory the FP64 kernels needed ~40 more registers and lost occupancy).  One
+// batch solves at a time per process (kq_batch_solve holds a lock); at most kMaxBatch systems.
 constexpr int kMaxBatch = 128;
 __constant__ SysDesc c_sys[kMaxBatch];
+__constant__ GroupDesc c_grp[kMaxBatch];
 
 // ---------------------------------------------------------------------------------------------------- helpers
 __device__ __forceinline__ bool tile_ticket_last(unsigned *ticket, int ntiles)
@@ -72,10 +84,35 @@ __device__ __forceinline__ double tile_partials_sum(const double *p, int n, doub
     return block_sum(s, sm);
 }
 
+// site of step s of this thread in tile `tile` (a tile is spt x BS consecutive sites)
+template <int BS>
+__device__ __forceinline__ int tile_site(int tile, int spt, int s)
+{
+    return (tile * spt + s) * BS + threadIdx.x;
+}
+
+// members of group G whose system iterates with operator precision M in this launch (uniform over the CTA: the
+// states only change in the scalar steps, which run after every tile of the system has passed)
+template <int R, int M>
+__device__ __forceinline__ unsigned group_mask(const GroupDesc &G)
+{
+    unsigned use = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        if (r < G.n) {
+            const MsState *st = c_sys[G.mem[r]].st;
+            if (st->active && st->mode == M) use |= 1u << r;
+        }
+    return use;
+}
+
+// operator-precision members per pass: the FP64 accumulators of more than 4 right-hand sides would not fit the
+// registers next to an FP64 link, so an FP64 group of 8 runs in two passes of 4 (links loaded twice)
+template <int M, int R> struct Pass { static constexpr int v = (M == 0 && R > 4) ? 4 : R; };
+
 // ---------------------------------------------------------------------------------------------------- kernels
 template <int BS>
-__global__ void __launch_bounds__(BS) bk_init_kernel(const SysDesc *__restrict__ sys, const int2 *__restrict__ items,
-                                                     int nitems)
+__global__ void __launch_bounds__(BS) bk_init_kernel(const int2 *__restrict__ items, int nitems, int spt)
 {
     __shared__ double sm[32];
 #pragma unroll 1
@@ -83,9 +120,10 @@ __global__ void __launch_bounds__(BS) bk_init_kernel(const SysDesc *__restrict__
         const int2 w = items[it];
         const SysDesc &d = c_sys[w.x];
         MsState *st = d.st;
-        const int i = w.y * BS + threadIdx.x;
         double nn = 0.0;
-        if (i < d.g.vh) {
+        for (int sidx = 0; sidx < spt; ++sidx) {
+            const int i = tile_site<BS>(w.y, spt, sidx);
+            if (i >= d.g.vh) break;
             double v[6], z[6] = {0, 0, 0, 0, 0, 0};
             ld_spinor<0>(d.b, d.pv, i, v);
             st_spinor<0>(d.p0, d.pv, i, v);
@@ -132,96 +170,147 @@ __global__ void __launch_bounds__(BS) bk_init_kernel(const SysDesc *__restrict__
     }
 }
 
-// K1: tmp = D p0 and |tmp|^2 -> beta step with <p0, A p0> = sigma0 |p0|^2 + |tmp|^2 (|p0|^2 from the alpha step's
-// recurrence), for the systems whose operator precision is M (one launch per precision, so that each launch is
-// specialised; systems in the other precisions skip their items).  FP64 and HALF get up to 128 registers: at the
-// 85-register cap of three 256-thread CTAs per SM the long-link row rebuild and the HALF decode spill.
-template <int BS, int M>
-__global__ void __launch_bounds__(BS, (M == 1 ? 768 : 512) / BS) bk_dslash1_kernel(const SysDesc *__restrict__ sys,
-                                                        const int2 *__restrict__ items, int nitems)
+// Launch bounds of the dslash kernels: one group member (R = 1) keeps the single-system shapes (FP32: three
+// 256-thread CTAs per SM; FP64 and HALF up to 128 registers, at the 85-register cap the long-link row rebuild and
+// the HALF decode spill); several members need room for their accumulators (FP64: one 256-thread CTA per SM).
+template <int BS, int M, int R> struct Bounds {
+    static constexpr int v = R == 1 ? (M == 1 ? 768 : 512) / BS : (M == 0 ? 256 : 512) / BS;
+};
+
+// K1: tmp_r = D p0_r and |tmp_r|^2 -> beta step with <p0, A p0> = sigma0 |p0|^2 + |tmp|^2 (|p0|^2 from the alpha
+// step's recurrence), for the members of each group whose operator precision is M (one launch per precision, so
+// that each launch is specialised; members in the other precisions are skipped).
+template <int BS, int M, int R>
+__global__ void __launch_bounds__(BS, Bounds<BS, M, R>::v) bk_dslash1_kernel(const int2 *__restrict__ items,
+                                                                            int nitems, int spt)
 {
     typedef typename Acc2<M, M>::T T;
+    constexpr int RP = Pass<M, R>::v;
     __shared__ double sm[32];
 #pragma unroll 1
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const int2 w = items[it];
-        const SysDesc &d = c_sys[w.x];
-        MsState *st = d.st;
-        if (!st->active || st->mode != M) continue;
-        const int i = w.y * BS + threadIdx.x;
-        double tt = 0.0;
-        if (i < d.g.vh) {
-            T acc[6];
-            dslash_site_t<M, 0, T>(d.g, d.pv, d.fat[M], d.lng[M], d.p0, 1 - d.parity, i, acc);
-            st_spinor_as<M>(d.tmp, d.pv, i, acc);
+        const GroupDesc &G = c_grp[w.x];
+        const unsigned use = group_mask<R, M>(G);
+        if (!use) continue;
+        const SysDesc &d0 = c_sys[G.mem[0]];
+        double tt[R];
 #pragma unroll
-            for (int k = 0; k < 6; ++k) tt += (double)acc[k] * (double)acc[k];
-        }
-        tt = block_sum(tt, sm);
-        if (threadIdx.x == 0) d.partials[w.y] = tt;
-        if (tile_ticket_last(&st->ticket[1], d.ntiles)) {
-            const double tot = tile_partials_sum(d.partials, d.ntiles, sm);
-            if (threadIdx.x < 32) {
-                ms_step_beta(st, st->shift[0] * st->pp + __shfl_sync(0xffffffffu, tot, 0));
-                if (threadIdx.x == 0) st->ticket[1] = 0;
+        for (int r = 0; r < R; ++r) tt[r] = 0.0;
+        for (int sidx = 0; sidx < spt; ++sidx) {
+            const int i = tile_site<BS>(w.y, spt, sidx);
+            if (i >= d0.g.vh) break;
+#pragma unroll
+            for (int base = 0; base < R; base += RP) {
+                const unsigned u = (use >> base) & ((1u << RP) - 1u);
+                if (!u) continue;
+                T acc[RP][6];
+                dslash_site_mrhs_t<M, 0, T, RP>(d0.g, d0.pv, d0.fat[M], d0.lng[M],
+                                                static_cast<const char *>(d0.p0) + base * d0.vb, d0.vb, u,
+                                                1 - d0.parity, i, acc);
+#pragma unroll
+                for (int r = 0; r < RP; ++r)
+                    if (u & (1u << r)) {
+                        st_spinor_as<M>(static_cast<char *>(d0.tmp) + (base + r) * d0.vb, d0.pv, i, acc[r]);
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) tt[base + r] += (double)acc[r][k] * (double)acc[r][k];
+                    }
             }
         }
-        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (use & (1u << r)) {
+                const SysDesc &d = c_sys[G.mem[r]];
+                MsState *st = d.st;
+                const double bt = block_sum(tt[r], sm);
+                if (threadIdx.x == 0) d.partials[w.y] = bt;
+                if (tile_ticket_last(&st->ticket[1], d.ntiles)) {
+                    const double tot = tile_partials_sum(d.partials, d.ntiles, sm);
+                    if (threadIdx.x < 32) {
+                        ms_step_beta(st, st->shift[0] * st->pp + __shfl_sync(0xffffffffu, tot, 0));
+                        if (threadIdx.x == 0) st->ticket[1] = 0;
+                    }
+                }
+                __syncthreads();
+            }
     }
 }
 
-// K2: r^(i+1) = r^(i) + B0 (sigma0 p0 - D tmp) into the ring (s stays in registers), |r|^2 -> alpha step, for the
-// systems in precision M.  The alpha step picks the next iteration's precision in next_mode, applied in K3, so the
-// K2 launches of the other precisions in this iteration do not pick the system up again.
-template <int BS, int M>
-__global__ void __launch_bounds__(BS, (M == 1 ? 768 : 512) / BS) bk_dslash2_kernel(const SysDesc *__restrict__ sys,
-                                                        const int2 *__restrict__ items, int nitems)
+// K2: r_r^(i+1) = r_r^(i) + B0 (sigma0 p0_r - D tmp_r) into each member's ring (s stays in registers), |r_r|^2 ->
+// alpha step, for the members in precision M.  The alpha step picks the next iteration's precision in next_mode,
+// applied in K3, so the K2 launches of the other precisions in this iteration do not pick the system up again.
+template <int BS, int M, int R>
+__global__ void __launch_bounds__(BS, Bounds<BS, M, R>::v) bk_dslash2_kernel(const int2 *__restrict__ items,
+                                                                            int nitems, int spt)
 {
     typedef typename Acc2<M, M>::T T;
+    constexpr int RP = Pass<M, R>::v;
     __shared__ double sm[32];
 #pragma unroll 1
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const int2 w = items[it];
-        const SysDesc &d = c_sys[w.x];
-        MsState *st = d.st;
-        if (!st->active || st->mode != M) continue;
-        const int itc = st->iter;
-        const char *rin = static_cast<const char *>(d.ring) + (size_t)(itc % kWin) * d.vb;
-        char *rout = static_cast<char *>(d.ring) + (size_t)((itc + 1) % kWin) * d.vb;
-        const int i = w.y * BS + threadIdx.x;
-        double nn = 0.0;
-        if (i < d.g.vh) {
-            T acc[6];
-            dslash_site_t<M, M, T>(d.g, d.pv, d.fat[M], d.lng[M], d.tmp, d.parity, i, acc);
-            double pv6[6], rv[6];
-            ld_spinor<0>(d.p0, d.pv, i, pv6);
-            ld_spinor<0>(rin, d.pv, i, rv);
-            const double sig = st->shift[0], b0 = st->B[0];
+        const GroupDesc &G = c_grp[w.x];
+        const unsigned use = group_mask<R, M>(G);
+        if (!use) continue;
+        const SysDesc &d0 = c_sys[G.mem[0]];
+        double nn[R];
 #pragma unroll
-            for (int k = 0; k < 6; ++k) {
-                rv[k] += b0 * (sig * pv6[k] - (double)acc[k]);
-                nn += rv[k] * rv[k];
+        for (int r = 0; r < R; ++r) nn[r] = 0.0;
+        for (int sidx = 0; sidx < spt; ++sidx) {
+            const int i = tile_site<BS>(w.y, spt, sidx);
+            if (i >= d0.g.vh) break;
+#pragma unroll
+            for (int base = 0; base < R; base += RP) {
+                const unsigned u = (use >> base) & ((1u << RP) - 1u);
+                if (!u) continue;
+                T acc[RP][6];
+                dslash_site_mrhs_t<M, M, T, RP>(d0.g, d0.pv, d0.fat[M], d0.lng[M],
+                                                static_cast<const char *>(d0.tmp) + base * d0.vb, d0.vb, u,
+                                                d0.parity, i, acc);
+#pragma unroll
+                for (int r = 0; r < RP; ++r)
+                    if (u & (1u << r)) {
+                        const SysDesc &d = c_sys[G.mem[base + r]];
+                        const MsState *st = d.st;
+                        const int itc = st->iter;
+                        const char *rin = static_cast<const char *>(d.ring) + (size_t)(itc % kWin) * d.vb;
+                        char *rout = static_cast<char *>(d.ring) + (size_t)((itc + 1) % kWin) * d.vb;
+                        double pv6[6], rv[6];
+                        ld_spinor<0>(d.p0, d.pv, i, pv6);
+                        ld_spinor<0>(rin, d.pv, i, rv);
+                        const double sig = st->shift[0], b0 = st->B[0];
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) {
+                            rv[k] += b0 * (sig * pv6[k] - (double)acc[r][k]);
+                            nn[base + r] += rv[k] * rv[k];
+                        }
+                        st_spinor<0>(rout, d.pv, i, rv);
+                    }
             }
-            st_spinor<0>(rout, d.pv, i, rv);
         }
-        nn = block_sum(nn, sm);
-        if (threadIdx.x == 0) d.partials[w.y] = nn;
-        if (tile_ticket_last(&st->ticket[2], d.ntiles)) {
-            const double tot = tile_partials_sum(d.partials, d.ntiles, sm);
-            if (threadIdx.x < 32) {
-                ms_step_alpha(st, __shfl_sync(0xffffffffu, tot, 0));
-                if (threadIdx.x == 0) st->ticket[2] = 0;
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (use & (1u << r)) {
+                const SysDesc &d = c_sys[G.mem[r]];
+                MsState *st = d.st;
+                const double bn = block_sum(nn[r], sm);
+                if (threadIdx.x == 0) d.partials[w.y] = bn;
+                if (tile_ticket_last(&st->ticket[2], d.ntiles)) {
+                    const double tot = tile_partials_sum(d.partials, d.ntiles, sm);
+                    if (threadIdx.x < 32) {
+                        ms_step_alpha(st, __shfl_sync(0xffffffffu, tot, 0));
+                        if (threadIdx.x == 0) st->ticket[2] = 0;
+                    }
+                }
+                __syncthreads();
             }
-        }
-        __syncthreads();
     }
 }
 
 // K3: p0 = r^(i) + a0 p0; the next iteration's precision takes effect.  A system that stopped in K2 no longer
 // needs p0.
 template <int BS>
-__global__ void __launch_bounds__(BS) bk_p0_kernel(const SysDesc *__restrict__ sys, const int2 *__restrict__ items,
-                                                   int nitems)
+__global__ void __launch_bounds__(BS) bk_p0_kernel(const int2 *__restrict__ items, int nitems, int spt)
 {
 #pragma unroll 1
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
@@ -229,13 +318,14 @@ __global__ void __launch_bounds__(BS) bk_p0_kernel(const SysDesc *__restrict__ s
         const SysDesc &d = c_sys[w.x];
         MsState *st = d.st;
         if (!st->active) continue;
-        const int i = w.y * BS + threadIdx.x;
-        if (i < d.g.vh) {
-            const char *r = static_cast<const char *>(d.ring) + (size_t)(st->iter % kWin) * d.vb;
+        const char *r = static_cast<const char *>(d.ring) + (size_t)(st->iter % kWin) * d.vb;
+        const double a0 = st->a[0];
+        for (int sidx = 0; sidx < spt; ++sidx) {
+            const int i = tile_site<BS>(w.y, spt, sidx);
+            if (i >= d.g.vh) break;
             double rv[6], pv6[6];
             ld_spinor<0>(r, d.pv, i, rv);
             ld_spinor<0>(d.p0, d.pv, i, pv6);
-            const double a0 = st->a[0];
 #pragma unroll
             for (int k = 0; k < 6; ++k) pv6[k] = rv[k] + a0 * pv6[k];
             st_spinor<0>(d.p0, d.pv, i, pv6);
@@ -250,8 +340,7 @@ __global__ void __launch_bounds__(BS) bk_p0_kernel(const SysDesc *__restrict__ s
 
 // K4: windowed shift update of every system that iterated in this window
 template <int BS>
-__global__ void __launch_bounds__(BS) bk_window_kernel(const SysDesc *__restrict__ sys,
-                                                       const int2 *__restrict__ items, int nitems)
+__global__ void __launch_bounds__(BS) bk_window_kernel(const int2 *__restrict__ items, int nitems, int spt)
 {
     __shared__ double sc[kMaxShift], se[kMaxShift], sd[kMaxShift][kWin], sf[kMaxShift][kWin];
 #pragma unroll 1
@@ -272,10 +361,12 @@ __global__ void __launch_bounds__(BS) bk_window_kernel(const SysDesc *__restrict
             }
         }
         __syncthreads();
-        const int i = w.y * BS + threadIdx.x;
-        if (i < d.g.vh)
+        for (int sidx = 0; sidx < spt; ++sidx) {
+            const int i = tile_site<BS>(w.y, spt, sidx);
+            if (i >= d.g.vh) break;
             window_update_site(static_cast<const char *>(d.ring), d.vb, d.pv, i, n, kmax, sc, se, sd, sf,
                                static_cast<char *>(d.pw), static_cast<char *>(d.x));
+        }
         if (tile_ticket_last(&st->ticket[0], d.ntiles)) {
             if (threadIdx.x == 0) {
                 st->wpos = 0;
@@ -287,25 +378,44 @@ __global__ void __launch_bounds__(BS) bk_window_kernel(const SysDesc *__restrict
 }
 
 // ---------------------------------------------------------------------------------------------------- host
+// items: per-system (system, tile) items for init / p0 / window, per-group (group, tile) items for the dslash steps
+struct BatchItems {
+    const int2 *sys;
+    int nsys;
+    const int2 *grp;
+    int ngrp;
+};
+
 template <int BS>
-static void enqueue_batch_init(const SysDesc *d, const int2 *items, int nitems, int grid, cudaStream_t s)
+static void enqueue_batch_init(const BatchItems &it, int grid, int spt, cudaStream_t s)
 {
-    bk_init_kernel<BS><<<grid, BS, 0, s>>>(d, items, nitems);
+    bk_init_kernel<BS><<<grid, BS, 0, s>>>(it.sys, it.nsys, spt);
+}
+
+template <int BS, int R>
+static void enqueue_batch_chunk_r(const BatchItems &it, int grid, int spt, cudaStream_t s)
+{
+    for (int k = 0; k < kChunk; ++k) {
+        bk_dslash1_kernel<BS, 0, R><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
+        bk_dslash1_kernel<BS, 1, R><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
+        bk_dslash1_kernel<BS, 2, R><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
+        bk_dslash2_kernel<BS, 0, R><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
+        bk_dslash2_kernel<BS, 1, R><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
+        bk_dslash2_kernel<BS, 2, R><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
+        bk_p0_kernel<BS><<<grid, BS, 0, s>>>(it.sys, it.nsys, spt);
+    }
+    bk_window_kernel<BS><<<grid, BS, 0, s>>>(it.sys, it.nsys, spt);
 }
 
 template <int BS>
-static void enqueue_batch_chunk(const SysDesc *d, const int2 *items, int nitems, int grid, cudaStream_t s)
+static void enqueue_batch_chunk(const BatchItems &it, int grid, int rhs, int spt, cudaStream_t s)
 {
-    for (int it = 0; it < kChunk; ++it) {
-        bk_dslash1_kernel<BS, 0><<<grid, BS, 0, s>>>(d, items, nitems);
-        bk_dslash1_kernel<BS, 1><<<grid, BS, 0, s>>>(d, items, nitems);
-        bk_dslash1_kernel<BS, 2><<<grid, BS, 0, s>>>(d, items, nitems);
-        bk_dslash2_kernel<BS, 0><<<grid, BS, 0, s>>>(d, items, nitems);
-        bk_dslash2_kernel<BS, 1><<<grid, BS, 0, s>>>(d, items, nitems);
-        bk_dslash2_kernel<BS, 2><<<grid, BS, 0, s>>>(d, items, nitems);
-        bk_p0_kernel<BS><<<grid, BS, 0, s>>>(d, items, nitems);
+    switch (rhs) {
+        case 8: enqueue_batch_chunk_r<BS, 8>(it, grid, spt, s); break;
+        case 4: enqueue_batch_chunk_r<BS, 4>(it, grid, spt, s); break;
+        case 2: enqueue_batch_chunk_r<BS, 2>(it, grid, spt, s); break;
+        default: enqueue_batch_chunk_r<BS, 1>(it, grid, spt, s); break;
     }
-    bk_window_kernel<BS><<<grid, BS, 0, s>>>(d, items, nitems);
 }
 
 }  // namespace kq
@@ -329,9 +439,8 @@ struct kq_batch {
     size_t work_bytes = 0;
     int *d_running = nullptr;
     int *h_running = nullptr;  // pinned
-    SysDesc *d_desc = nullptr;
-    int2 *d_items = nullptr;
-    size_t items_cap = 0, desc_cap = 0;
+    int2 *d_items = nullptr;   // per-system items, then per-group items
+    size_t items_cap = 0;
 };
 
 #define KQ_API extern "C" __attribute__((visibility("default")))
@@ -361,7 +470,6 @@ KQ_API void kq_batch_destroy(kq_batch *b)
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->work) cudaFree(b->work);
-    if (b->d_desc) cudaFree(b->d_desc);
     if (b->d_items) cudaFree(b->d_items);
     if (b->d_running) cudaFree(b->d_running);
     if (b->h_running) cudaFreeHost(b->h_running);
@@ -426,74 +534,117 @@ namespace {
 
 struct BatchPlan {
     std::vector<SysDesc> desc;
-    std::vector<int2> items;
+    std::vector<GroupDesc> groups;
+    std::vector<int2> sys_items, grp_items;
     std::vector<MsState> init;
 };
 
-// Lay out every system's buffers in the batch workspace and build descriptors, work items and initial states.
-cudaError_t batch_plan(kq_batch *b, int bs, BatchPlan &plan, bool carve_only, size_t *bytes)
+// Systems on the same context (gauge field) and parity, in batch order, in groups of at most rhs members.
+std::vector<GroupDesc> form_groups(const std::vector<BatchSystem> &sys, int rhs)
+{
+    std::vector<GroupDesc> groups;
+    std::vector<int> open;  // index of the group each system's (context, parity) currently fills, -1 if none
+    for (size_t si = 0; si < sys.size(); ++si) {
+        int gi = -1;
+        for (size_t g = 0; g < groups.size(); ++g) {
+            const BatchSystem &m = sys[groups[g].mem[0]];
+            if (m.ctx == sys[si].ctx && m.param.parity == sys[si].param.parity && groups[g].n < rhs) gi = (int)g;
+        }
+        if (gi < 0) {
+            GroupDesc G;
+            memset(&G, 0, sizeof(G));
+            groups.push_back(G);
+            gi = (int)groups.size() - 1;
+        }
+        groups[gi].mem[groups[gi].n++] = (int)si;
+    }
+    return groups;
+}
+
+// largest number of systems sharing one context and parity (the most right-hand sides a link load can serve)
+int max_shared(const std::vector<BatchSystem> &sys)
+{
+    int best = 0;
+    for (const GroupDesc &G : form_groups(sys, kMaxR)) best = std::max(best, G.n);
+    return best;
+}
+
+// Lay out every system's buffers in the batch workspace and build descriptors, groups, work items and initial
+// states.  A tile is spt x bs consecutive sites.
+cudaError_t batch_plan(kq_batch *b, int bs, int rhs, int spt, BatchPlan &plan, bool carve_only, size_t *bytes)
 {
     Carve c(carve_only ? nullptr : b->work);
-    plan.desc.clear();
-    plan.items.clear();
-    plan.init.clear();
-    for (size_t si = 0; si < b->sys.size(); ++si) {
-        BatchSystem &S = b->sys[si];
-        kq_context *ctx = S.ctx;
-        const Geom &g = ctx->g;
-        const int ns = S.param.num_shift;
-        SysDesc d;
-        memset(&d, 0, sizeof(d));
-        d.g = g;
-        d.pv = pad_sites(g.vh);
-        d.parity = S.param.parity;
-        d.ntiles = (g.vh + bs - 1) / bs;
-        for (int p = 0; p < 3; ++p) {
-            d.fat[p] = ctx->gd.fat[p];
-            d.lng[p] = ctx->gd.lng[p];
-        }
+    plan.desc.assign(b->sys.size(), SysDesc{});
+    plan.init.assign(b->sys.size(), MsState{});
+    plan.sys_items.clear();
+    plan.grp_items.clear();
+    plan.groups = form_groups(b->sys, rhs);
+    const int tile = bs * spt;
+    for (size_t gi = 0; gi < plan.groups.size(); ++gi) {
+        const GroupDesc &G = plan.groups[gi];
+        const Geom &g = b->sys[G.mem[0]].ctx->g;
         const size_t vb = spinor_bytes(g, P64);
-        d.vb = vb;
-        d.b = S.d_b;
-        d.x = S.d_x;
-        d.p0 = c.take(vb);
-        d.tmp = c.take(vb);
-        d.ring = c.take(vb * kWin);
-        d.pw = c.take(vb * ns);
-        d.partials = static_cast<double *>(c.take(sizeof(double) * d.ntiles));
-        d.st = static_cast<MsState *>(c.take(sizeof(MsState)));
-        plan.desc.push_back(d);
-        for (int t = 0; t < d.ntiles; ++t) plan.items.push_back(make_int2((int)si, t));
-        MsState h;
-        memset(&h, 0, sizeof(h));
-        h.ns = ns;
-        h.max_iter = S.param.max_iter > 0 ? S.param.max_iter : 100000;
-        std::vector<double> sig(ns);
-        for (int k = 0; k < ns; ++k)
-            sig[k] = (S.param.shift_mode == 0 && k > 0) ? S.shifts[0] + S.shifts[k] : S.shifts[k];
-        h.shift[0] = sig[0];
-        for (int k = 1; k < ns; ++k) h.shift[k] = sig[k] - sig[0];
-        if (S.param.solver == KQ_SOLVER_MIXED) {
-            // the single-system mixed solver's schedule (kq_mixed.cu): stop at 0.7 x target, FP32 from
-            // 0.3 target / 3e-7, HALF from 0.3 target / 1e-3
-            const double tgt = S.param.rel_residual > 0 ? S.param.rel_residual : 1e-10;
-            h.tol = -0.7 * tgt;  // relative: the init kernel turns it into (0.7 tgt |b|)^2
-            const double r32 = 0.3 * tgt / 3e-7, r16 = 0.3 * tgt / 1e-3;
-            h.rho32_2 = r32 * r32;
-            h.rho16_2 = prec_from_api(S.param.prec) == P16 ? r16 * r16 : 0.0;
-        } else {
-            h.tol = S.param.tol;
+        const int ntiles = (g.vh + tile - 1) / tile;
+        // the group's p0 and tmp fields are consecutive (the multi-RHS dslash addresses member r at base + r vb)
+        char *p0 = static_cast<char *>(c.take(vb * G.n));
+        char *tmp = static_cast<char *>(c.take(vb * G.n));
+        for (int t = 0; t < ntiles; ++t) plan.grp_items.push_back(make_int2((int)gi, t));
+        for (int r = 0; r < G.n; ++r) {
+            const int si = G.mem[r];
+            BatchSystem &S = b->sys[si];
+            kq_context *ctx = S.ctx;
+            const int ns = S.param.num_shift;
+            SysDesc &d = plan.desc[si];
+            memset(&d, 0, sizeof(d));
+            d.g = g;
+            d.pv = pad_sites(g.vh);
+            d.parity = S.param.parity;
+            d.ntiles = ntiles;
+            for (int p = 0; p < 3; ++p) {
+                d.fat[p] = ctx->gd.fat[p];
+                d.lng[p] = ctx->gd.lng[p];
+            }
+            d.vb = vb;
+            d.b = S.d_b;
+            d.x = S.d_x;
+            d.p0 = p0 ? p0 + r * vb : nullptr;
+            d.tmp = tmp ? tmp + r * vb : nullptr;
+            d.ring = c.take(vb * kWin);
+            d.pw = c.take(vb * ns);
+            d.partials = static_cast<double *>(c.take(sizeof(double) * ntiles));
+            d.st = static_cast<MsState *>(c.take(sizeof(MsState)));
+            MsState &h = plan.init[si];
+            memset(&h, 0, sizeof(h));
+            h.ns = ns;
+            h.max_iter = S.param.max_iter > 0 ? S.param.max_iter : 100000;
+            std::vector<double> sig(ns);
+            for (int k = 0; k < ns; ++k)
+                sig[k] = (S.param.shift_mode == 0 && k > 0) ? S.shifts[0] + S.shifts[k] : S.shifts[k];
+            h.shift[0] = sig[0];
+            for (int k = 1; k < ns; ++k) h.shift[k] = sig[k] - sig[0];
+            if (S.param.solver == KQ_SOLVER_MIXED) {
+                // the single-system mixed solver's schedule (kq_mixed.cu): stop at 0.7 x target, FP32 from
+                // 0.3 target / 3e-7, HALF from 0.3 target / 1e-3
+                const double tgt = S.param.rel_residual > 0 ? S.param.rel_residual : 1e-10;
+                h.tol = -0.7 * tgt;  // relative: the init kernel turns it into (0.7 tgt |b|)^2
+                const double r32 = 0.3 * tgt / 3e-7, r16 = 0.3 * tgt / 1e-3;
+                h.rho32_2 = r32 * r32;
+                h.rho16_2 = prec_from_api(S.param.prec) == P16 ? r16 * r16 : 0.0;
+            } else {
+                h.tol = S.param.tol;
+            }
+            h.running = b->d_running;
         }
-        h.running = b->d_running;
-        plan.init.push_back(h);
     }
+    for (size_t si = 0; si < b->sys.size(); ++si)
+        for (int t = 0; t < plan.desc[si].ntiles; ++t) plan.sys_items.push_back(make_int2((int)si, t));
     *bytes = c.off;
     return cudaSuccess;
 }
 
 }  // namespace
 
-static std::mutex g_batch_mu;  // the descriptor table in constant memory is shared by all batches
+static std::mutex g_batch_mu;  // the descriptor tables in constant memory are shared by all batches
 
 // The batched iterations over every system in b->sys, then each system's FP64 check / refinement.
 static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
@@ -502,25 +653,42 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
     cudaStream_t s = b->stream;
     int dev_sms = 148;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, b->device);
+    const int shared = max_shared(b->sys);
 
-    // launch shape: tuned once per batch signature (sizes, shifts, schedule), cached on disk
-    std::string key = "batch";
-    for (auto &S : b->sys)
+    // launch shape: tuned once per batch signature (sizes, shared gauge fields, shifts, schedule), cached on disk
+    std::string key = "batch2";
+    for (auto &S : b->sys) {
+        int owner = 0;  // first system on the same context: systems sharing links share this number
+        while (b->sys[owner].ctx != S.ctx) ++owner;
         key += "_" + std::to_string(S.ctx->g.n[0]) + "x" + std::to_string(S.ctx->g.n[1]) + "x" +
-               std::to_string(S.ctx->g.n[2]) + "x" + std::to_string(S.ctx->g.n[3]) + "s" +
-               std::to_string(S.param.num_shift) + "m" + std::to_string(S.param.solver) + "p" +
+               std::to_string(S.ctx->g.n[2]) + "x" + std::to_string(S.ctx->g.n[3]) + "c" + std::to_string(owner) +
+               "s" + std::to_string(S.param.num_shift) + "m" + std::to_string(S.param.solver) + "p" +
                std::to_string(S.param.prec);
+    }
     BatchTune tune;
-    const bool have_tune = tune_lookup(key, &tune);
+    bool have_tune = tune_lookup(key, &tune);
+    // KUQCD_BATCH_SHAPE="threads,ctas_per_sm,rhs,sites_per_thread" fixes the shape (no tuning, no cache)
+    if (const char *shape = getenv("KUQCD_BATCH_SHAPE")) {
+        BatchTune t{256, 4, 1, 1};
+        if (sscanf(shape, "%d,%d,%d,%d", &t.bs, &t.ctas_per_sm, &t.rhs, &t.spt) == 4 && (t.bs == 128 || t.bs == 256) &&
+            t.ctas_per_sm >= 1 && t.ctas_per_sm <= 32 && (t.rhs == 1 || t.rhs == 2 || t.rhs == 4 || t.rhs == 8) &&
+            (t.spt == 1 || t.spt == 2)) {
+            tune = t;
+            have_tune = true;
+        }
+    }
     if (!have_tune) {
         tune.bs = 256;
         tune.ctas_per_sm = 4;
+        tune.rhs = 1;
+        tune.spt = 1;
     }
 
-    auto run = [&](int bs, int cps, int max_chunks, float *ms_out, long long *launches, int *chunks_out) -> cudaError_t {
+    auto run = [&](const BatchTune &t, int max_chunks, float *ms_out, long long *launches, int *chunks_out,
+                   int *ngroups) -> cudaError_t {
         BatchPlan plan;
         size_t bytes = 0;
-        batch_plan(b, bs, plan, true, &bytes);
+        batch_plan(b, t.bs, t.rhs, t.spt, plan, true, &bytes);
         if (b->work_bytes < bytes) {
             if (b->work) cudaFree(b->work);
             b->work = nullptr;
@@ -528,39 +696,41 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
             KQ_CUDA_TRY(cudaMalloc(&b->work, bytes));
             b->work_bytes = bytes;
         }
-        batch_plan(b, bs, plan, false, &bytes);
-        const size_t nsys = plan.desc.size(), nit = plan.items.size();
-        if (b->desc_cap < nsys) {
-            if (b->d_desc) cudaFree(b->d_desc);
-            KQ_CUDA_TRY(cudaMalloc(&b->d_desc, sizeof(SysDesc) * nsys));
-            b->desc_cap = nsys;
-        }
-        if (b->items_cap < nit) {
+        batch_plan(b, t.bs, t.rhs, t.spt, plan, false, &bytes);
+        const size_t nsys = plan.desc.size(), nsi = plan.sys_items.size(), ngi = plan.grp_items.size();
+        if (b->items_cap < nsi + ngi) {
             if (b->d_items) cudaFree(b->d_items);
-            KQ_CUDA_TRY(cudaMalloc(&b->d_items, sizeof(int2) * nit));
-            b->items_cap = nit;
+            b->d_items = nullptr;
+            KQ_CUDA_TRY(cudaMalloc(&b->d_items, sizeof(int2) * (nsi + ngi)));
+            b->items_cap = nsi + ngi;
         }
-        KQ_CUDA_TRY(cudaMemcpyAsync(b->d_desc, plan.desc.data(), sizeof(SysDesc) * nsys, cudaMemcpyHostToDevice, s));
         KQ_CUDA_TRY(cudaMemcpyToSymbolAsync(c_sys, plan.desc.data(), sizeof(SysDesc) * nsys, 0,
                                             cudaMemcpyHostToDevice, s));
-        KQ_CUDA_TRY(cudaMemcpyAsync(b->d_items, plan.items.data(), sizeof(int2) * nit, cudaMemcpyHostToDevice, s));
+        KQ_CUDA_TRY(cudaMemcpyToSymbolAsync(c_grp, plan.groups.data(), sizeof(GroupDesc) * plan.groups.size(), 0,
+                                            cudaMemcpyHostToDevice, s));
+        KQ_CUDA_TRY(cudaMemcpyAsync(b->d_items, plan.sys_items.data(), sizeof(int2) * nsi, cudaMemcpyHostToDevice,
+                                    s));
+        KQ_CUDA_TRY(cudaMemcpyAsync(b->d_items + nsi, plan.grp_items.data(), sizeof(int2) * ngi,
+                                    cudaMemcpyHostToDevice, s));
         for (size_t i = 0; i < nsys; ++i)
             KQ_CUDA_TRY(cudaMemcpyAsync(plan.desc[i].st, &plan.init[i], sizeof(MsState), cudaMemcpyHostToDevice, s));
         const int nsys_i = (int)nsys;
         KQ_CUDA_TRY(cudaMemcpyAsync(b->d_running, &nsys_i, sizeof(int), cudaMemcpyHostToDevice, s));
-        const int grid = std::max(1, std::min((int)nit, dev_sms * cps));
+        const BatchItems items{b->d_items, (int)nsi, b->d_items + nsi, (int)ngi};
+        const int grid = std::max(1, std::min((int)nsi, dev_sms * t.ctas_per_sm));
+        *ngroups = (int)plan.groups.size();
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
-        if (bs == 128) enqueue_batch_init<128>(b->d_desc, b->d_items, (int)nit, grid, s);
-        else enqueue_batch_init<256>(b->d_desc, b->d_items, (int)nit, grid, s);
+        if (t.bs == 128) enqueue_batch_init<128>(items, grid, t.spt, s);
+        else enqueue_batch_init<256>(items, grid, t.spt, s);
         KQ_CUDA_TRY(cudaGetLastError());
         *launches = 1;
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         KQ_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        if (bs == 128) enqueue_batch_chunk<128>(b->d_desc, b->d_items, (int)nit, grid, s);
-        else enqueue_batch_chunk<256>(b->d_desc, b->d_items, (int)nit, grid, s);
+        if (t.bs == 128) enqueue_batch_chunk<128>(items, grid, t.rhs, t.spt, s);
+        else enqueue_batch_chunk<256>(items, grid, t.rhs, t.spt, s);
         cudaError_t ee = cudaStreamEndCapture(s, &graph);
         if (ee == cudaSuccess) ee = cudaGraphInstantiate(&exec, graph, 0);
         if (graph) cudaGraphDestroy(graph);
@@ -590,29 +760,51 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
     };
 
     if (!have_tune) {
-        // time two windows of the real batch for every candidate shape; the solve restarts afterwards
+        // Time two windows of the real batch per candidate shape (the solve restarts afterwards), one dimension
+        // at a time: tile x CTAs per SM with every shared gauge field serving as many right-hand sides as it can,
+        // then the right-hand sides per CTA, then the sites per thread.
         float best = 1e30f;
+        auto trial = [&](BatchTune t) -> cudaError_t {
+            float ms = 0;
+            long long l = 0;
+            int ch = 0, ng = 0;
+            const cudaError_t e = run(t, 2, &ms, &l, &ch, &ng);
+            if (e == cudaSuccess && ch > 0 && ms < best) {
+                best = ms;
+                tune = t;
+            }
+            return e;
+        };
+        int rmax = 1;
+        while (rmax < std::min(shared, kMaxR)) rmax *= 2;
+        BatchTune t{256, 4, rmax, 1};
         const int bss[2] = {128, 256}, cpss[4] = {2, 4, 8, 16};
         for (int bs : bss)
             for (int cps : cpss) {
                 if (bs == 256 && cps > 8) continue;
-                float ms = 0;
-                long long l = 0;
-                int ch = 0;
-                cudaError_t e = run(bs, cps, 2, &ms, &l, &ch);
+                t.bs = bs;
+                t.ctas_per_sm = cps;
+                const cudaError_t e = trial(t);
                 if (e != cudaSuccess) return status_of(e);
-                if (ch > 0 && ms < best) {
-                    best = ms;
-                    tune.bs = bs;
-                    tune.ctas_per_sm = cps;
-                }
             }
+        t = tune;
+        for (int r = 1; r <= rmax; r *= 2) {
+            if (r == t.rhs) continue;
+            BatchTune c = t;
+            c.rhs = r;
+            const cudaError_t e = trial(c);
+            if (e != cudaSuccess) return status_of(e);
+        }
+        BatchTune c = tune;
+        c.spt = 2;
+        const cudaError_t e = trial(c);
+        if (e != cudaSuccess) return status_of(e);
         tune_store(key, tune);
     }
     float ms = 0;
     long long launches = 0;
-    int chunks = 0;
-    cudaError_t e = run(tune.bs, tune.ctas_per_sm, 0, &ms, &launches, &chunks);
+    int chunks = 0, ngroups = 0;
+    cudaError_t e = run(tune, 0, &ms, &launches, &chunks, &ngroups);
     if (e != cudaSuccess) {
         set_last_error(std::string("kq_batch_solve: ") + cudaGetErrorString(e));
         return status_of(e);
@@ -620,7 +812,7 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
     // per-system results, then the FP64 check / refinement of the mixed systems
     BatchPlan plan;
     size_t bytes = 0;
-    batch_plan(b, tune.bs, plan, false, &bytes);
+    batch_plan(b, tune.bs, tune.rhs, tune.spt, plan, false, &bytes);
     int refined = 0;
     double worst = 0.0;
     int maxit = 0;
@@ -669,14 +861,18 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
         out->max_true_residual = worst;
         out->refined_systems = refined;
         out->tuned_now = have_tune ? 0 : 1;
+        out->rhs_per_cta = tune.rhs;
+        out->sites_per_thread = tune.spt;
+        out->groups = ngroups;
     }
     return KUQCD_SUCCESS;
 }
 
 // Systems of at least this many sites per parity fill the GPU on their own, and the single-system solver (kernels
 // specialised for one lattice, no per-item mode checks) runs them faster than the batched kernels (measured on
-// B200: 24^3 x 48 and 32^4 systems 10-16 % faster one after another); smaller systems are batched.  Override with
-// KUQCD_BATCH_LARGE_SITES.
+// B200: 24^3 x 48 and 32^4 systems 10-16 % faster one after another); smaller systems are batched.  A large system
+// that shares its gauge field with another system of the batch stays batched: there the grouped dslash loads each
+// link once for all of them.  Override with KUQCD_BATCH_LARGE_SITES.
 static int large_sites()
 {
     const char *e = getenv("KUQCD_BATCH_LARGE_SITES");
@@ -705,7 +901,11 @@ KQ_API KuQCDStatus kq_batch_solve(kq_batch *b, kq_batch_info *out)
     }
     const int big = large_sites();
     std::vector<int> large, small;
-    for (size_t i = 0; i < b->sys.size(); ++i) (b->sys[i].ctx->g.vh >= big ? large : small).push_back((int)i);
+    for (size_t i = 0; i < b->sys.size(); ++i) {
+        int sharing = 0;
+        for (const BatchSystem &o : b->sys) sharing += (o.ctx == b->sys[i].ctx) ? 1 : 0;
+        (b->sys[i].ctx->g.vh >= big && sharing == 1 ? large : small).push_back((int)i);
+    }
     if (large.empty()) return solve_batched(b, out);
 
     // the small systems, batched, in a helper thread on the batch's stream; meanwhile the large ones one after
@@ -754,6 +954,9 @@ KQ_API KuQCDStatus kq_batch_solve(kq_batch *b, kq_batch_info *out)
         out->max_true_residual = std::max(worst, bi.max_true_residual);
         out->refined_systems = refined + bi.refined_systems;
         out->tuned_now = bi.tuned_now;
+        out->rhs_per_cta = bi.rhs_per_cta;
+        out->sites_per_thread = bi.sites_per_thread;
+        out->groups = bi.groups + (int)large.size();
     }
     if (st_small != KUQCD_SUCCESS) {
         set_last_error(err_small);

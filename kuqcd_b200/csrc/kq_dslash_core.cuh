@@ -275,6 +275,64 @@ __device__ __forceinline__ void dslash_site_mrhs(const Geom &g, int pv, const Li
     for (int r = 0; r < R; ++r) fold_scale_site<LP>(fat, acc[r]);
 }
 
+// Multi-RHS form with the input fields in any storage precision SP and arithmetic in T (the batched solver's
+// grouped systems: R systems on one gauge field, fields at src0 + r * stride).  The links of site i are loaded
+// once per call and applied to every right-hand side r with use & (1 << r).
+template <int LP, int SP, typename T, int R>
+__device__ __forceinline__ void dslash_site_mrhs_t(const Geom &g, int pv, const LinkSet &fat, const LinkSet &lng,
+                                                   const char *src0, size_t stride, unsigned use, int p, int i,
+                                                   T acc[R][6])
+{
+    const SiteCoord c = site_coord(g, i, p);
+    const void *fat_p = p ? fat.par[1] : fat.par[0], *fat_q = p ? fat.par[0] : fat.par[1];
+    const void *lng_p = p ? lng.par[1] : lng.par[0], *lng_q = p ? lng.par[0] : lng.par[1];
+    const T rl = fold_scale_long<LP, T>(fat, lng);
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) acc[r][k] = T(0);
+#pragma unroll
+    for (int dir = 0; dir < 4; ++dir) {
+        const int nf1 = nbr_index(g, c, i, dir, 1);
+        const int nf3 = nbr_index(g, c, i, dir, 3);
+        const int nb1 = nbr_index(g, c, i, dir, -1);
+        const int nb3 = nbr_index(g, c, i, dir, -3);
+        T u[18], v[6];
+        ld_link_fold<LP>(fat_p, pv, dir, i, fat, u);
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (use & (1u << r)) {
+                ld_spinor_as<SP>(src0 + r * stride, pv, nf1, v);
+                mv_add(u, v, acc[r]);
+            }
+        ld_link_fold<LP>(lng_p, pv, dir, i, lng, u);
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (use & (1u << r)) {
+                ld_spinor_as<SP>(src0 + r * stride, pv, nf3, v);
+                fold_long_spinor<LP>(rl, v);
+                mv_add(u, v, acc[r]);
+            }
+        ld_link_fold<LP>(fat_q, pv, dir, nb1, fat, u);
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (use & (1u << r)) {
+                ld_spinor_as<SP>(src0 + r * stride, pv, nb1, v);
+                mdv_sub(u, v, acc[r]);
+            }
+        ld_link_fold<LP>(lng_q, pv, dir, nb3, lng, u);
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (use & (1u << r)) {
+                ld_spinor_as<SP>(src0 + r * stride, pv, nb3, v);
+                fold_long_spinor<LP>(rl, v);
+                mdv_sub(u, v, acc[r]);
+            }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) fold_scale_site<LP>(fat, acc[r]);
+}
+
 // ------------------------------------------------------------------------------------------------ reductions
 // Deterministic block sum of a double (fixed shuffle tree, then warp 0 over the per-warp sums).
 __device__ __forceinline__ double block_sum(double v, double *smem32)

@@ -21,6 +21,7 @@
 
 #include "kq_internal.h"
 #include "kq_solver.h"
+#define KUQCD_NO_CLASS_API  // the five calls only; the class-level API is header-only for callers
 #include "kuqcd.h"
 
 #define KQ_API extern "C" __attribute__((visibility("default")))

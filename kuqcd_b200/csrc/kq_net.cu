@@ -270,6 +270,13 @@ KuQCDStatus prepare(kq_net *n)
 
 }  // namespace
 
+// ptc_check_fault reports a tile whose bounded wait ran out as cudaErrorLaunchTimeout
+static const char *net_error_text(cudaError_t e)
+{
+    return e == cudaErrorLaunchTimeout ? "a tensor-core tile did not complete within the wait limit"
+                                       : cudaGetErrorString(e);
+}
+
 // kernels one kq_net_apply launches once its BF16 matrices are built: embed, 2 x nl layers, extract
 int net_apply_launches(const kq_net *n) { return n ? 2 + 2 * n->nl : 0; }
 
@@ -285,7 +292,7 @@ KQ_API KuQCDStatus kq_net_apply(kq_net *n, const void *d_in, void *d_out, int pa
     cudaError_t e = forward(n, d_in, parity, 1.0);
     if (e == cudaSuccess) e = ptc_extract(n->ctx->g, n->cact[0], parity, d_out, 1.0, n->ctx->stream);
     if (e == cudaSuccess) e = ptc_check_fault(n->ctx->stream);
-    if (e != cudaSuccess) set_last_error(std::string("kq_net_apply: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) set_last_error(std::string("kq_net_apply: ") + net_error_text(e));
     return status_of(e);
 }
 
@@ -335,7 +342,7 @@ KQ_API KuQCDStatus kq_net_train_pair(kq_net *n, const void *d_r, const void *d_e
     }
     if (e == cudaSuccess) e = ptc_check_fault(s);
     if (loss) *loss = l;
-    if (e != cudaSuccess) set_last_error(std::string("kq_net_train_pair: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) set_last_error(std::string("kq_net_train_pair: ") + net_error_text(e));
     return status_of(e);
 }
 

@@ -8,8 +8,10 @@
 namespace kq {
 
 struct BatchTune {
-    int bs;           // threads per CTA = sites per tile
+    int bs;           // threads per CTA
     int ctas_per_sm;  // resident CTAs per SM of the persistent grid
+    int rhs;          // right-hand sides per CTA: systems on one gauge field that share each link load (1,2,4,8)
+    int spt;          // sites per thread: a tile is spt x bs sites
 };
 
 bool tune_lookup(const std::string &key, BatchTune *out);

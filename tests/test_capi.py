@@ -119,3 +119,14 @@ def test_context_argument_checks():
     assert lib.kq_context_create((C.c_uint * 4)(3, 4, 4, 4), 0, C.byref(h)) == K.KUQCD_ERR_INVALID_PARAM
     assert lib.kq_dslash(None, 8, None, None, 0, None) == K.KUQCD_ERR_NULL_POINTER
     assert lib.kq_solve_multishift(None, None, None, None, None) == K.KUQCD_ERR_NULL_POINTER
+
+
+@pytest.mark.parametrize("caller", ["caller_kuqcd", "caller_classes"])
+def test_cpp_callers_compile_against_include_and_link(tmp_path, caller):
+    """include/kuqcd.h and the class-level headers it brings in compile warning-free (-Wall -Wextra -Werror) in a
+    C++ caller, and the caller links against libkuqcd_b200.so (the mangled kuqcd:: symbols and the C ABI)."""
+    cmd = ["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-Werror", "-I", str(ROOT / "include"),
+           str(ROOT / "tests" / "cpp" / f"{caller}.cpp"), "-L", str(ROOT / "kuqcd_b200"), "-lkuqcd_b200",
+           "-o", str(tmp_path / caller)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]

@@ -123,3 +123,85 @@ def test_batch_with_large_systems_on_the_single_system_solver(cuda, tmp_path, mo
             r = O.true_residual(dims, fat, lng, parity, s, b, xk)
             assert r <= 1.2e-10, (i, k, r)
     batch.close()
+
+
+def sources_on_one_field(dims, eps, seed, n, parity=0):
+    """n systems on one gauge field: own Gaussian source and own mass each (one context, so the batch groups them
+    and its dslash loads every link once for all members)."""
+    fat, lng = O.make_links(dims, eps, seed)
+    ctx = K.Context(dims)
+    ctx.load_links(K.KUQCD_FAT_LINK, fat)
+    ctx.load_links(K.KUQCD_LONG_LINK, lng)
+    vb = ctx.spinor_bytes(K.KUQCD_DOUBLE)
+    rng = np.random.default_rng(seed)
+    out = []
+    for j in range(n):
+        b = O.make_source(dims, parity, seed * 100 + j)
+        d_b = torch.zeros(vb, dtype=torch.uint8, device="cuda")
+        ctx.upload(K.KUQCD_DOUBLE, b, d_b)
+        mass = float(rng.uniform(0.01, 0.1))
+        ns = int(rng.integers(4, 13))
+        out.append((b, d_b, list(mass * mass + np.logspace(-4, 0, ns))))
+    return ctx, fat, lng, vb, out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("solver,prec", [(K.KQ_SOLVER_MIXED, K.KUQCD_HALF),
+                                         (K.KQ_SOLVER_CGM_WINDOWED, K.KUQCD_DOUBLE)])
+def test_batch_many_sources_on_one_field_match_single_system(cuda, tmp_path, monkeypatch, solver, prec):
+    """8 sources (own masses and shift sets) on one 16^4 gauge field, batched with the grouped multi-RHS dslash,
+    against the single-system solver on each: solutions within 1e-9, true residuals within target; the tuner
+    searched the right-hand sides per CTA and the sites per thread."""
+    monkeypatch.setenv("KUQCD_TUNE_CACHE", str(tmp_path / "tune.txt"))
+    dims = (16, 16, 16, 16)
+    ctx, fat, lng, vb, systems = sources_on_one_field(dims, 0.3, 21, 8)
+    batch = K.Batch()
+    xs = []
+    for b, d_b, sig in systems:
+        d_x = torch.zeros(vb * len(sig), dtype=torch.uint8, device="cuda")
+        batch.add(ctx, d_b, d_x, sig, solver=solver, prec=prec, rel_residual=1e-10,
+                  tol=(1e-10) ** 2 * float(b @ b))
+        xs.append(d_x)
+    info = batch.solve()
+    assert info.num_systems == 8 and info.rhs_per_cta in (1, 2, 4, 8) and info.sites_per_thread in (1, 2)
+    assert info.groups == (8 + info.rhs_per_cta - 1) // info.rhs_per_cta
+    for j, (b, d_b, sig) in enumerate(systems):
+        assert batch.system_info(j).status == 0, j
+        ref, single = ctx.solve(b, sig, parity=0, solver=solver, prec=prec, rel_residual=1e-10,
+                                tol=(1e-10) ** 2 * float(b @ b))
+        if solver == K.KQ_SOLVER_CGM_WINDOWED:
+            assert abs(batch.system_info(j).iter - single.iter) <= 1, j
+        for k, s in enumerate(sig):
+            xb = ctx.download(K.KUQCD_DOUBLE, xs[j][k * vb:(k + 1) * vb])
+            r = O.true_residual(dims, fat, lng, 0, s, b, xb)
+            assert r <= (1.2e-10 if solver == K.KQ_SOLVER_MIXED else 1.5e-10), (j, k, r)
+            assert np.abs(xb - ref[k]).max() <= 1e-9 * np.abs(ref[k]).max(), (j, k)
+    batch.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rhs,spt", [(1, 1), (2, 2), (4, 1), (8, 2)])
+def test_batch_groups_of_every_width(cuda, monkeypatch, rhs, spt):
+    """Every right-hand-sides-per-CTA width, set through KUQCD_BATCH_SHAPE, on groups that do not fill it: 3 sources
+    on one field (odd parity), 2 on another lattice, one system alone; all reach their targets."""
+    monkeypatch.setenv("KUQCD_BATCH_SHAPE", f"256,2,{rhs},{spt}")
+    batch = K.Batch()
+    keep = []
+    for dims, eps, seed, n, parity in [((8, 8, 8, 8), 0.3, 31, 3, 1), ((8, 4, 4, 8), 0.35, 32, 2, 0),
+                                       ((6, 6, 6, 6), 0.25, 33, 1, 0)]:
+        ctx, fat, lng, vb, systems = sources_on_one_field(dims, eps, seed, n, parity)
+        for b, d_b, sig in systems:
+            d_x = torch.zeros(vb * len(sig), dtype=torch.uint8, device="cuda")
+            batch.add(ctx, d_b, d_x, sig, parity=parity, solver=K.KQ_SOLVER_MIXED, prec=K.KUQCD_HALF,
+                      rel_residual=1e-10)
+            keep.append((ctx, fat, lng, vb, b, d_x, sig, parity, dims))
+    info = batch.solve()
+    assert info.tuned_now == 0 and info.rhs_per_cta == rhs and info.sites_per_thread == spt
+    assert info.groups == sum((n + rhs - 1) // rhs for n in (3, 2, 1))
+    for i, (ctx, fat, lng, vb, b, d_x, sig, parity, dims) in enumerate(keep):
+        assert batch.system_info(i).status == 0, i
+        for k, s in enumerate(sig):
+            xk = ctx.download(K.KUQCD_DOUBLE, d_x[k * vb:(k + 1) * vb])
+            r = O.true_residual(dims, fat, lng, parity, s, b, xk)
+            assert r <= 1.2e-10, (i, k, r)
+    batch.close()
