@@ -658,12 +658,13 @@ def run_batch(args, shared=False):
     def sequential():
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        worst, iters = 0.0, 0
+        worst, iters, refine = 0.0, 0, 0
         for ctx, d_b, d_x, sig, dims in systems:
             inf = ctx.solve_device(d_b, d_x, sig, solver=K.KQ_SOLVER_MIXED, prec=prec, rel_residual=REL_RES)
             worst = max(worst, max(inf.true_residual[:len(sig)]))
             iters = max(iters, inf.iter)
-        return time.perf_counter() - t0, worst, iters
+            refine += inf.iter_refine
+        return time.perf_counter() - t0, worst, iters, refine
 
     for _ in range(args.warmup):
         batched()
@@ -687,8 +688,11 @@ def run_batch(args, shared=False):
                    "tile": info.tile, "ctas_per_sm": info.ctas_per_sm, "rhs_per_cta": info.rhs_per_cta,
                    "sites_per_thread": info.sites_per_thread, "groups": info.groups,
                    "max_iterations": info.iterations, "refined_systems": info.refined_systems,
+                   "refine_iterations": info.refine_iterations,
+                   "batched_phase_ms": info.batched_seconds * 1e3, "check_refine_ms": info.check_seconds * 1e3,
                    "max_true_residual": bt[-1][2]},
-        "sequential": {"ms_per_step": t_s * 1e3, "max_true_residual": st[-1][1], "speedup_of_batched": t_s / t_b},
+        "sequential": {"ms_per_step": t_s * 1e3, "max_true_residual": st[-1][1], "refine_iterations": st[-1][3],
+                       "speedup_of_batched": t_s / t_b},
         "gpu_launches": int(info.kernel_launches), "clocks": clk.summary(),
     }
     print(json.dumps(res))

@@ -225,6 +225,8 @@ typedef struct {
     int rhs_per_cta;          /* systems on one gauge field whose dslash shares each link load (1, 2, 4 or 8) */
     int sites_per_thread;     /* sites each thread handles per work item */
     int groups;               /* groups of systems sharing link loads (+ systems solved on their own) */
+    double check_seconds;     /* wall time of the batched systems' FP64 checks and refinements */
+    int refine_iterations;    /* refinement iterations summed over the batched systems */
 } kq_batch_info;
 
 KuQCDStatus kq_batch_create(int device, kq_batch **out);

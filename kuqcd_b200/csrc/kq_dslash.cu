@@ -2,7 +2,10 @@
 // sigma - D_pq D_qp, MdaggM + Axmy of inverter_cgm.cpp:45-46).  One thread per output site; links are
 // streamed from HBM once, neighbour spinors come through L1/L2.  Link and spinor precisions are independent
 // template parameters (FP64/FP64, FP32/FP32, HALF/HALF, HALF links with FP32 spinors).
+#include <cstdlib>
+
 #include "kq_dslash_core.cuh"
+#include "kq_dslash_half2.cuh"
 
 namespace kq {
 
@@ -59,6 +62,16 @@ __global__ void __launch_bounds__(256) dslash_full_kernel(Geom g, int pv, LinkSe
     st_spinor<SP>(dst + p * half, pv, i, acc);
 }
 
+// KUQCD_HALF_DSLASH=site selects the one-site-per-thread HALF kernel instead of the two-site packed one
+static bool half_pairs()
+{
+    static const bool pairs = [] {
+        const char *e = getenv("KUQCD_HALF_DSLASH");
+        return !(e && e[0] == 's');
+    }();
+    return pairs;
+}
+
 static bool pair_ok(int lp, int sp)
 {
     return (lp == sp) || (lp == P16 && sp == P32);
@@ -77,9 +90,16 @@ cudaError_t launch_dslash2(const Geom &g, const GaugeDev &gd, int lp, int sp, co
         set_last_error("dslash: links not resident in the requested precision, or unsupported precision pair");
         return cudaErrorInvalidValue;
     }
+    const int pv = pad_sites(g.vh);
+    if (lp == P16 && sp == P16 && !gate && half_pairs()) {
+        // HALF: two sites per thread in packed FP32 (kq_dslash_half2.cuh)
+        constexpr int kBS2 = 128;
+        const int nb2 = (g.vh + 2 * kBS2 - 1) / (2 * kBS2);
+        dslash_half2_kernel<kBS2><<<nb2, kBS2, 0, s>>>(g, pv, gd.fat[lp], gd.lng[lp], src, dst, dst_parity);
+        return cudaGetLastError();
+    }
     const int bs = block > 0 ? block : 256;
     const int nb = (g.vh + bs - 1) / bs;
-    const int pv = pad_sites(g.vh);
     KQ_DISPATCH_PAIR(lp, sp, (dslash_kernel<LP, SP><<<nb, bs, 0, s>>>(g, pv, gd.fat[lp], gd.lng[lp], src, dst,
                                                                        dst_parity, gate)));
     return cudaGetLastError();

@@ -566,6 +566,7 @@ cudaError_t mixed_solve(::kq_context *ctx, const kq_solve_param *param, const do
     int *poll = reinterpret_cast<int *>(ctx->poll);
     cudaError_t err = cudaSuccess;
     int replays = 0;
+    const int hs_max_iter = param->max_iter > 0 ? param->max_iter : 100000;
     for (;;) {
         KQ_CUDA_TRY(cudaMemcpyAsync(poll, mw.st, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
         err = cudaStreamSynchronize(s);
@@ -573,7 +574,7 @@ cudaError_t mixed_solve(::kq_context *ctx, const kq_solve_param *param, const do
         err = cudaGraphLaunch(exec, s);
         if (err != cudaSuccess) break;
         launches += 7LL * chunk;
-        if (++replays > 1000000) break;
+        if (++replays > hs_max_iter / chunk + 8) break;  // the refinement stops by then while its state is consistent
     }
     cudaGraphExecDestroy(exec);
     KQ_CUDA_TRY(err);

@@ -280,6 +280,15 @@ static const char *net_error_text(cudaError_t e)
 // kernels one kq_net_apply launches once its BF16 matrices are built: embed, 2 x nl layers, extract
 int net_apply_launches(const kq_net *n) { return n ? 2 + 2 * n->nl : 0; }
 
+// d_out = M(d_in) enqueued on the context's stream without waiting for it: the caller checks the tensor-core
+// fault word later (ptc_check_fault), once for many applications (the FCG polish, once per chunk of iterations)
+cudaError_t net_apply_async(kq_net *n, const void *d_in, void *d_out, int parity)
+{
+    if (prepare(n) != KUQCD_SUCCESS) return cudaErrorInvalidValue;
+    KQ_CUDA_TRY(forward(n, d_in, parity, 1.0));
+    return ptc_extract(n->ctx->g, n->cact[0], parity, d_out, 1.0, n->ctx->stream);
+}
+
 // d_out = M(d_in) on `parity` (FP64 fields of the context's layout)
 KQ_API KuQCDStatus kq_net_apply(kq_net *n, const void *d_in, void *d_out, int parity)
 {

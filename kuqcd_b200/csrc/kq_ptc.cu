@@ -21,6 +21,7 @@
 #include <cuda_bf16.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -176,9 +177,11 @@ __global__ void __launch_bounds__(kThr) ptc_forward_kernel(Geom g, int pv, LinkS
     unsigned char *Bs = As + 3 * A_BYTES;          // [kNT x KP]
     uint64_t *mbar = reinterpret_cast<uint64_t *>(Bs + kNT * KP * 2);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
-    const int tiles_per_par = (g.vh + kTile - 1) / kTile;
-    const int par = blockIdx.x / tiles_per_par;
-    const int base = (blockIdx.x - par * tiles_per_par) * kTile;
+    // tiles in parity-interleaved order (block 2j: tile j of parity 0, block 2j + 1: tile j of parity 1): the two
+    // uses of every link (forward hop at its site, backward hop at the neighbour) and of every activation (own
+    // site, eight neighbours) then fall close together in time and the second one hits L2
+    const int par = blockIdx.x & 1;
+    const int base = (blockIdx.x >> 1) * kTile;
     const int t = threadIdx.x, warp = t >> 5;
     if (warp == 0) umma::tmem_alloc(tslot, kTmemCols);
     if (t == 0) {
@@ -232,6 +235,160 @@ __global__ void __launch_bounds__(kThr) ptc_forward_kernel(Geom g, int pv, LinkS
     if (warp == 0) umma::tmem_dealloc(tbase, kTmemCols);
 }
 
+// Forward layer with 8 input channels, K-chunked by path: K = 9 paths x 16 columns, and each path's 16 columns of
+// the gathered tile are one K = 16 step of the MMA.  The CTA gathers path j into one of two chunk buffers while the
+// tensor cores multiply chunk j - 1 from the other, so shared memory holds 2 x 3 x [128 x 16] BF16 (24 KB) instead
+// of the whole [128 x 144] tile per colour (108 KB): five or more CTAs fit on an SM and hide each other's gather
+// latency.  Chunk j's MMAs commit to mbarrier (j & 1); before chunk j + 2 overwrites that buffer every thread waits
+// for the commit's phase (j >> 1) & 1 (bounded, as in the whole-tile kernel).
+constexpr uint32_t kChunkColBytes = kTile * 16 * 2;  // one colour's [128 x 16] BF16 chunk
+template <int COUT>
+__global__ void __launch_bounds__(kThr, 4) ptc_forward8_kernel(Geom g, int pv, LinkSet fat, const float2 *__restrict__ in,
+                                                            float2 *__restrict__ out, const __nv_bfloat16 *__restrict__ Bt,
+                                                            int swap_paths, int *fault)
+{
+    constexpr int CIN = 8, KP = kpad_of(CIN), NP = npad_of(COUT);
+    constexpr uint32_t CH_BYTES = 3 * kChunkColBytes;  // one chunk: 3 colours
+    constexpr uint32_t SBO_A = (16 / 8) * 128, SBO_B = (KP / 8) * 128;
+    static_assert(KP == kPaths * 16 && NP <= kNT, "one path per K step");
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char *Ach = smem_raw;                  // [2][3][kChunkColBytes]
+    unsigned char *Bs = Ach + 2 * CH_BYTES;         // [kNT x KP]
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(Bs + kNT * KP * 2);  // [2]
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 2);
+    const int par = blockIdx.x & 1;  // parity-interleaved tile order (see ptc_forward_kernel)
+    const int base = (blockIdx.x >> 1) * kTile;
+    const int t = threadIdx.x, warp = t >> 5;
+    if (warp == 0) umma::tmem_alloc(tslot, kTmemCols);
+    if (t == 0) {
+        umma::mbar_init(&mbar[0], 1);
+        umma::mbar_init(&mbar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int e = t; e < kNT * KP; e += kThr) {
+        const int n = e / KP, k = e - n * KP;
+        *reinterpret_cast<__nv_bfloat16 *>(Bs + umma::kmajor_offset(n, k, KP)) =
+            n < NP ? Bt[n * KP + k] : __float2bfloat16_rn(0.f);
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tbase = *tslot;
+    const int i = base + t;
+    const bool valid = i < g.vh;
+    const SiteCoord cd = site_coord(g, valid ? i : 0, par);
+    const int q = 1 - par;
+    const void *fat_p = par ? fat.par[1] : fat.par[0];
+    const void *fat_q = par ? fat.par[0] : fat.par[1];
+    constexpr uint32_t idesc = umma::idesc_bf16_f32(kTile, kNT);
+    const uint32_t a0 = umma::smem_u32(Ach), b0 = umma::smem_u32(Bs);
+    bool ok = true;
+#pragma unroll 1
+    for (int j = 0; j < kPaths && ok; ++j) {
+        const int buf = j & 1;
+        if (j >= 2) {  // the MMAs of chunk j - 2 must be done reading this buffer
+            ok = __syncthreads_and(umma::mbar_wait(&mbar[buf], ((j - 2) >> 1) & 1, kWaitLimit));
+            if (!ok) break;
+            umma::fence_after_sync();
+        }
+        // path j: identity, then for each direction the forward and the backward hop
+        int p = 0;
+        float vals[3][2 * CIN];
+        if (j == 0) {
+#pragma unroll
+            for (int c = 0; c < CIN; ++c)
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    const float2 v = valid ? ld_act(in, pv, c, par, a, i) : make_float2(0.f, 0.f);
+                    vals[a][2 * c] = v.x;
+                    vals[a][2 * c + 1] = v.y;
+                }
+        } else {
+            const int dir = (j - 1) >> 1, fb = (j - 1) & 1;
+            p = 1 + 2 * dir + (swap_paths ? 1 - fb : fb);
+            if (valid) {
+                const int nb = nbr_index(g, cd, i, dir, fb == 0 ? 1 : -1);
+                float u[18];
+                ld_link<1>(fb == 0 ? fat_p : fat_q, pv, dir, fb == 0 ? i : nb, 1.f, u);
+#pragma unroll
+                for (int c = 0; c < CIN; ++c) {
+                    float v[6], o[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        const float2 w = ld_act(in, pv, c, q, a, nb);
+                        v[2 * a] = w.x;
+                        v[2 * a + 1] = w.y;
+                    }
+                    if (fb == 0) mv_add(u, v, o);
+                    else {
+                        mdv_sub(u, v, o);
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) o[k] = -o[k];
+                    }
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        vals[a][2 * c] = o[2 * a];
+                        vals[a][2 * c + 1] = o[2 * a + 1];
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int k = 0; k < 2 * CIN; ++k) vals[a][k] = 0.f;
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            unsigned char *col = Ach + buf * CH_BYTES + a * kChunkColBytes;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint4 w;
+                w.x = pack_bf16(vals[a][8 * h + 0], vals[a][8 * h + 1]);
+                w.y = pack_bf16(vals[a][8 * h + 2], vals[a][8 * h + 3]);
+                w.z = pack_bf16(vals[a][8 * h + 4], vals[a][8 * h + 5]);
+                w.w = pack_bf16(vals[a][8 * h + 6], vals[a][8 * h + 7]);
+                *reinterpret_cast<uint4 *>(col + umma::kmajor_offset(t, 8 * h, 16)) = w;
+            }
+        }
+        umma::fence_smem_to_async();
+        umma::fence_before_sync();
+        __syncthreads();
+        umma::fence_after_sync();
+        if (t == 0) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                umma::mma_bf16(tbase + a * kNT, umma::smem_desc(a0 + buf * CH_BYTES + a * kChunkColBytes, SBO_A),
+                               umma::smem_desc(b0 + p * 256, SBO_B), idesc, j > 0 ? 1u : 0u);
+            umma::mma_commit(&mbar[buf]);
+        }
+    }
+    // the last two chunks (7 on buffer 1, 8 on buffer 0) complete their barriers' phases 1 and 0
+    if (ok) ok = __syncthreads_and(umma::mbar_wait(&mbar[1], 1, kWaitLimit) && umma::mbar_wait(&mbar[0], 0, kWaitLimit));
+    if (!ok) {
+        if (t == 0) atomicExch(fault, 1);
+        // give the MMAs in flight a last chance before freeing their memory
+        umma::mbar_wait(&mbar[0], 0, kWaitLimit);
+        umma::mbar_wait(&mbar[1], 1, kWaitLimit);
+    }
+    umma::fence_after_sync();
+    if (ok) {
+#pragma unroll 1
+        for (int a = 0; a < 3; ++a) {
+            float d[16];
+            umma::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + a * kNT, d);
+            if (valid) {
+#pragma unroll
+                for (int o = 0; o < COUT; ++o)
+                    out[(size_t)((o * 2 + par) * 3 + a) * pv + i] = make_float2(d[2 * o], d[2 * o + 1]);
+            }
+        }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tbase, kTmemCols);
+}
+
 // ---------------------------------------------------------------------------------------------------- weight grad
 // partial[cta][k][n] = sum over the tiles this CTA visits (tile = blockIdx.x + j * gridDim.x) and over their rows
 // (sites x colours) of T[row][k] * G[row][n]  (swap_paths: T gathered as by the adjoint layer).
@@ -252,7 +409,7 @@ __global__ void __launch_bounds__(kThr) ptc_wgrad_kernel(Geom g, int pv, LinkSet
     unsigned char *Gs = As + 3 * A_BYTES;     // [3][G_BYTES]
     uint64_t *mbar = reinterpret_cast<uint64_t *>(Gs + 3 * G_BYTES);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
-    const int tiles_per_par = (g.vh + kTile - 1) / kTile, ntiles = 2 * tiles_per_par;
+    const int ntiles = 2 * ((g.vh + kTile - 1) / kTile);
     const int t = threadIdx.x, warp = t >> 5;
     if (warp == 0) umma::tmem_alloc(tslot, 32);
     if (t == 0) {
@@ -271,8 +428,8 @@ __global__ void __launch_bounds__(kThr) ptc_wgrad_kernel(Geom g, int pv, LinkSet
             if (!ok) break;
             umma::fence_after_sync();
         }
-        const int par = tile / tiles_per_par;
-        const int base = (tile - par * tiles_per_par) * kTile;
+        const int par = tile & 1;  // parity-interleaved tile order, as in the forward kernels
+        const int base = (tile >> 1) * kTile;
         gather_tile<CIN>(g, pv, fat, in, par, base, t, swap_paths != 0, As);
         const int i = base + t;
 #pragma unroll
@@ -408,7 +565,6 @@ __global__ void ptc_loss_kernel(int vh, int pv, const float2 *__restrict__ y, co
     if (threadIdx.x == 0) partials[blockIdx.x] = l;
 }
 
-// Adam on the real and imaginary parts of all weights
 // Adam on grad * grad_scale (the accumulated gradient of a batch times 1/batch); the accumulator is cleared here, so
 // the next batch starts from zero without a separate memset
 __global__ void ptc_adam_kernel(float *w, float *grad, float *m, float *v, int n, float lr, float grad_scale, float b1,
@@ -472,6 +628,20 @@ cudaError_t ptc_raise_fault_for_test()
     return cudaMemcpy(f, &one, sizeof(int), cudaMemcpyHostToDevice);
 }
 
+template <int COUT>
+static cudaError_t run_forward8(const Geom &g, const LinkSet &fat, const float2 *in, float2 *out,
+                                const __nv_bfloat16 *Bt, bool swap, cudaStream_t s)
+{
+    const int pv = pad_sites(g.vh);
+    const int tiles = 2 * ((g.vh + kTile - 1) / kTile);
+    const size_t sm = (size_t)2 * 3 * kChunkColBytes + (size_t)kNT * kpad_of(8) * 2 + 32;
+    KQ_CUDA_TRY(cudaFuncSetAttribute(ptc_forward8_kernel<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int *fault = fault_flag();
+    if (!fault) return cudaErrorInvalidDevicePointer;
+    ptc_forward8_kernel<COUT><<<tiles, kThr, sm, s>>>(g, pv, fat, in, out, Bt, swap ? 1 : 0, fault);
+    return cudaGetLastError();
+}
+
 template <int CIN, int COUT>
 static cudaError_t run_forward(const Geom &g, const LinkSet &fat, const float2 *in, float2 *out,
                                const __nv_bfloat16 *Bt, bool swap, cudaStream_t s)
@@ -514,8 +684,12 @@ cudaError_t ptc_forward(const Geom &g, const LinkSet &fat, int cin, int cout, co
 {
     const __nv_bfloat16 *B = static_cast<const __nv_bfloat16 *>(Bt);
     if (cin == 1 && cout == 8) return run_forward<1, 8>(g, fat, in, out, B, swap, s);
-    if (cin == 8 && cout == 8) return run_forward<8, 8>(g, fat, in, out, B, swap, s);
-    if (cin == 8 && cout == 1) return run_forward<8, 1>(g, fat, in, out, B, swap, s);
+    // 8 input channels: the K-chunked kernel (KUQCD_PTC_WHOLE_TILE=1 keeps the whole-tile one)
+    static const bool whole = getenv("KUQCD_PTC_WHOLE_TILE") && getenv("KUQCD_PTC_WHOLE_TILE")[0] == '1';
+    if (cin == 8 && cout == 8) return whole ? run_forward<8, 8>(g, fat, in, out, B, swap, s)
+                                            : run_forward8<8>(g, fat, in, out, B, swap, s);
+    if (cin == 8 && cout == 1) return whole ? run_forward<8, 1>(g, fat, in, out, B, swap, s)
+                                            : run_forward8<1>(g, fat, in, out, B, swap, s);
     if (cin == 1 && cout == 1) return run_forward<1, 1>(g, fat, in, out, B, swap, s);
     set_last_error("ptc: channel counts must be 1 or 8");
     return cudaErrorInvalidValue;

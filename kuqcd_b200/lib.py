@@ -80,7 +80,8 @@ class BatchInfo(C.Structure):
     _fields_ = [("num_systems", C.c_int), ("iterations", C.c_int), ("batched_seconds", C.c_double),
                 ("kernel_launches", C.c_longlong), ("tile", C.c_int), ("ctas_per_sm", C.c_int),
                 ("max_true_residual", C.c_double), ("refined_systems", C.c_int), ("tuned_now", C.c_int),
-                ("rhs_per_cta", C.c_int), ("sites_per_thread", C.c_int), ("groups", C.c_int)]
+                ("rhs_per_cta", C.c_int), ("sites_per_thread", C.c_int), ("groups", C.c_int),
+                ("check_seconds", C.c_double), ("refine_iterations", C.c_int)]
 
 _PKG = Path(__file__).resolve().parent
 lib_path = Path(os.environ.get("KUQCD_B200_LIB", _PKG / "libkuqcd_b200.so"))

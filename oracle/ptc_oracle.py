@@ -10,10 +10,26 @@ links of the host record scaled by 1/2 (the device copy the CUDA kernels read). 
 
 and the preconditioner is the Gram operator M = P^T N^dag N P of the chain N = L_{K-1} ... L_0 (P: embedding of
 one parity into a one-channel full-lattice field).
+
+With bf16=True every function rounds what the GPU rounds: the transported inputs T_p v (computed in FP32, then
+rounded to BF16 for the tensor cores), the weights (BF16 operands) and, in the weight gradient, the output gradient
+(BF16 operand of the gradient GEMM); sums stay exact (float64), as the tensor cores accumulate in FP32.  That
+oracle agrees with the GPU to FP32 accumulation error, so tests can hold the kernels to ~1e-4 instead of the
+few-parts-in-a-thousand gap between BF16 and exact arithmetic.
 """
 from __future__ import annotations
 
 import numpy as np
+
+
+def bf16(a):
+    """Round to the nearest BF16 (ties to even), through FP32 as the GPU does (float64 -> FP32 -> BF16); complex
+    arrays are rounded per real and imaginary part."""
+    if np.iscomplexobj(a):
+        return bf16(a.real) + 1j * bf16(a.imag)
+    u = np.asarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
 class Lattice:
@@ -60,24 +76,30 @@ class Lattice:
         return out
 
 
-def layer(lat, W, v):
+def _round(x, on):
+    return bf16(x) if on else x
+
+
+def layer(lat, W, v, bf=False):
     """W: (Cout, Cin, 9) complex; v: (Cin, 2, Vh, 3)."""
+    W = _round(W, bf)
     y = np.zeros((W.shape[0],) + v.shape[1:], dtype=complex)
     for c in range(W.shape[1]):
         ts = lat.transports(v[c])
         for p in range(9):
-            y += W[:, c, p][:, None, None, None] * ts[p][None]
+            y += W[:, c, p][:, None, None, None] * _round(ts[p], bf)[None]
     return y
 
 
-def layer_adjoint(lat, W, g):
+def layer_adjoint(lat, W, g, bf=False):
     """Adjoint of `layer`: T_fwd^dag = T_bwd and vice versa, weights conjugate-transposed."""
     swap = [0, 2, 1, 4, 3, 6, 5, 8, 7]
+    W = _round(W, bf)
     out = np.zeros((W.shape[1],) + g.shape[1:], dtype=complex)
     for o in range(W.shape[0]):
         ts = lat.transports(g[o])
         for p in range(9):
-            out += np.conj(W[o, :, p])[:, None, None, None] * ts[swap[p]][None]
+            out += np.conj(W[o, :, p])[:, None, None, None] * _round(ts[swap[p]], bf)[None]
     return out
 
 
@@ -108,38 +130,39 @@ def flat_from_weights(Ws):
     return np.concatenate([np.stack([W.real.ravel(), W.imag.ravel()], 1).ravel() for W in Ws])
 
 
-def _chains(lat, Ws, r, parity):
+def _chains(lat, Ws, r, parity, bf=False):
     """Forward chain a_0 = embed(r), a_{l+1} = L_l a_l and adjoint chain c_K = a_K, c_l = L_l^dag c_{l+1}."""
     acts = [embed(r, parity, lat.vh)]
     for W in Ws:
-        acts.append(layer(lat, W, acts[-1]))
+        acts.append(layer(lat, W, acts[-1], bf))
     cs = [None] * len(Ws) + [acts[-1]]
     for li in range(len(Ws) - 1, -1, -1):
-        cs[li] = layer_adjoint(lat, Ws[li], cs[li + 1])
+        cs[li] = layer_adjoint(lat, Ws[li], cs[li + 1], bf)
     return acts, cs
 
 
-def apply(lat, Ws, r, parity):
+def apply(lat, Ws, r, parity, bf=False):
     """M(r) = extract(N^dag N embed(r)), N = L_{K-1} ... L_0 (the Gram form kq_net.cu evaluates)."""
-    return extract(_chains(lat, Ws, r, parity)[1][0], parity)
+    return extract(_chains(lat, Ws, r, parity, bf)[1][0], parity)
 
 
-def _wgrad(lat, v, g, ncout, swap=False):
+def _wgrad(lat, v, g, ncout, swap=False, bf=False):
     """sum over sites and colours of g_o * conj(T_p v_c): the complex gradient of a layer's weights W[o, c, p]
     (swap: path labels of the adjoint layer)."""
     order = [0, 2, 1, 4, 3, 6, 5, 8, 7] if swap else list(range(9))
+    g = _round(g, bf)
     dW = np.zeros((ncout, v.shape[0], 9), dtype=complex)
     for c in range(v.shape[0]):
         ts = lat.transports(v[c])
         for p in range(9):
-            dW[:, c, p] = (g * np.conj(ts[order[p]])[None]).sum(axis=(1, 2, 3))
+            dW[:, c, p] = (g * np.conj(_round(ts[order[p]], bf))[None]).sum(axis=(1, 2, 3))
     return dW
 
 
-def loss_and_grad(lat, Ws, r, e, parity):
+def loss_and_grad(lat, Ws, r, e, parity, bf=False):
     """L = |M(r) - e|^2 / |e|^2 and dL/dW (complex, re part = dL/dW_re, im part = dL/dW_im) per layer; each layer
     collects one term through L_l and one through L_l^dag (whose weights are conj(W)^T, hence the conj)."""
-    acts, cs = _chains(lat, Ws, r, parity)
+    acts, cs = _chains(lat, Ws, r, parity, bf)
     y = extract(cs[0], parity)
     e2 = float(e @ e)
     L = float(((y - e) ** 2).sum()) / e2
@@ -150,12 +173,12 @@ def loss_and_grad(lat, Ws, r, e, parity):
     grads = [np.zeros_like(W) for W in Ws]
     for li in range(K):  # adjoint chain: g = dL/dc_li
         W = Ws[li]
-        dWa = _wgrad(lat, cs[li + 1], g, W.shape[1], swap=True)  # [i, o, p] of the adjoint layer
+        dWa = _wgrad(lat, cs[li + 1], g, W.shape[1], swap=True, bf=bf)  # [i, o, p] of the adjoint layer
         grads[li] += np.conj(dWa.transpose(1, 0, 2))
-        g = layer(lat, W, g)
+        g = layer(lat, W, g, bf)
     for li in range(K - 1, -1, -1):  # forward chain: g = dL/da_{li+1}
         W = Ws[li]
-        grads[li] += _wgrad(lat, acts[li], g, W.shape[0])
+        grads[li] += _wgrad(lat, acts[li], g, W.shape[0], bf=bf)
         if li > 0:
-            g = layer_adjoint(lat, W, g)
+            g = layer_adjoint(lat, W, g, bf)
     return L, grads

@@ -39,9 +39,50 @@ def test_net_forward_matches_oracle(cuda, parity):
     net.apply(a, z, parity)
     got = ctx.download(K.KUQCD_DOUBLE, z)
     lat = P.Lattice(dims, fat)
-    want = P.apply(lat, P.weights_from_flat(w.astype(np.float64), CH), r, parity)
-    # BF16 operands in four layers: a few parts in a thousand
+    Ws = P.weights_from_flat(w.astype(np.float64), CH)
+    want = P.apply(lat, Ws, r, parity)
+    # against exact arithmetic: BF16 operands in four layers, a few parts in a thousand
     assert np.linalg.norm(got - want) <= 3e-2 * np.linalg.norm(want)
+    # against the oracle that rounds the tensor-core operands as the kernels do: what is left are the few BF16
+    # roundings that an FP32 transported value and its FP64 counterpart take to different neighbours (up to 1.4e-4
+    # on this small lattice, measured on the oracle with FP32 transports) and FP32 accumulation; a wrong gather index
+    # in a single path would leave a relative error near 1/9, the BF16 operands themselves 1.6e-3
+    want16 = P.apply(lat, Ws, r, parity, bf=True)
+    assert np.linalg.norm(got - want16) <= 5e-4 * np.linalg.norm(want16)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("whole_tile", ["0", "1"])
+def test_net_forward_kernels_agree_on_a_ragged_lattice(cuda, monkeypatch, whole_tile):
+    """The K-chunked forward kernel of the 8-channel layers and the whole-tile kernel both match the BF16-rounding
+    oracle, on a lattice whose last tile is partly past the end (Vh = 1350 sites, 11 tiles of 128)."""
+    monkeypatch.setenv("KUQCD_PTC_WHOLE_TILE", whole_tile)
+    import subprocess
+    import sys
+    code = f"""
+import numpy as np, torch, kuqcd_b200 as K
+from oracle import oracle as O
+from oracle import ptc_oracle as P
+dims = (10, 6, 5, 9)
+fat, lng = O.make_links(dims, 0.35, 12)
+ctx = K.Context(dims)
+ctx.load_links(K.KUQCD_FAT_LINK, fat)
+ctx.load_links(K.KUQCD_LONG_LINK, lng)
+net = K.Net(ctx, (1, 8, 8))
+w = (0.3 * np.random.default_rng(3).standard_normal(net.nw)).astype(np.float32)
+net.weights = w
+r = O.make_source(dims, 1, 4)
+a = torch.zeros(ctx.spinor_bytes(K.KUQCD_DOUBLE), dtype=torch.uint8, device='cuda')
+z = torch.zeros_like(a)
+ctx.upload(K.KUQCD_DOUBLE, r, a)
+net.apply(a, z, 1)
+got = ctx.download(K.KUQCD_DOUBLE, z)
+want = P.apply(P.Lattice(dims, fat), P.weights_from_flat(w.astype(np.float64), (1, 8, 8)), r, 1, bf=True)
+print(float(np.linalg.norm(got - want) / np.linalg.norm(want)))
+"""
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-3000:]
+    assert float(out.stdout.strip().splitlines()[-1]) <= 2e-4
 
 
 @pytest.mark.gpu
@@ -78,15 +119,20 @@ def test_net_gradient_matches_oracle(cuda):
     loss = net.train_pair(dr, de, 0, float(e @ e))
     g = net.grad().astype(np.float64)
     lat = P.Lattice(dims, fat)
-    Lw, grads = P.loss_and_grad(lat, P.weights_from_flat(w.astype(np.float64), CH), r, e, 0)
+    Ws = P.weights_from_flat(w.astype(np.float64), CH)
+    Lw, grads = P.loss_and_grad(lat, Ws, r, e, 0)
     gw = P.flat_from_weights(grads)
     assert abs(loss - Lw) <= 3e-2 * Lw
     assert np.linalg.norm(g - gw) <= 5e-2 * np.linalg.norm(gw)
-    # per layer as well (the chain rule through the adjoint layers)
+    # against the oracle that rounds the tensor-core operands as the kernels do, per layer (the chain rule through
+    # the adjoint layers)
+    L16, grads16 = P.loss_and_grad(lat, Ws, r, e, 0, bf=True)
+    g16 = P.flat_from_weights(grads16)
+    assert abs(loss - L16) <= 1e-4 * L16
     off = 0
     for ci, co in zip(CH[:-1], CH[1:]):
         n = 2 * ci * co * 9
-        assert np.linalg.norm(g[off:off + n] - gw[off:off + n]) <= 6e-2 * np.linalg.norm(gw[off:off + n])
+        assert np.linalg.norm(g[off:off + n] - g16[off:off + n]) <= 2e-4 * np.linalg.norm(g16[off:off + n])
         off += n
 
 

@@ -82,3 +82,15 @@ def test_gradients_match_finite_differences():
         Lm = P.loss_and_grad(lat, P.weights_from_flat(fm, CH), r, e, 1)[0]
         fd = (Lp - Lm) / (2 * h)
         assert abs(fd - gflat[k]) <= 1e-6 * max(1.0, abs(fd)), (k, fd, gflat[k])
+
+
+def test_bf16_mode_rounds_the_tensor_core_operands():
+    """bf16 rounds to nearest with ties to even (through FP32, as the GPU converts), and the BF16-operand network
+    differs from the exact one by a few parts in a thousand -- the gap the exact-oracle tolerances allow for."""
+    x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8, 1.0 + 2 ** -9, -3.14159, 0.0])
+    assert list(P.bf16(x)) == [1.0, 1.0, 1.0 + 2 ** -6, 1.0, -3.140625, 0.0]
+    lat, Ws, rng = setup(3)
+    u = O.make_source(DIMS, 0, 13)
+    exact, rounded = P.apply(lat, Ws, u, 0), P.apply(lat, Ws, u, 0, bf=True)
+    rel = np.linalg.norm(rounded - exact) / np.linalg.norm(exact)
+    assert 1e-5 < rel < 3e-2
