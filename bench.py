@@ -602,10 +602,11 @@ def run_reference(args):
 
 
 def run_batch(args, shared=False):
-    """Batched multi-system workload: 24 systems, 8 each on 16^4, 24^3x48 and 32^4, own mass (m ~ U[0.01,0.1]),
-    8-16 shifts log-spaced 1e-4..1 and Gaussian source, all seeded; every system has its own gauge field
-    (eps ~ U[0.2,0.4]) -- or, with shared=True (--config batch-rhs), the 8 systems of each lattice share one gauge
-    field (many sources and masses on one configuration), so the grouped dslash loads each link once for all of them.
+    """Batched multi-system workload: 24 systems, 8 each on 16^4, 24^3x48 and 32^4, own gauge field
+    (eps ~ U[0.2,0.4]), own mass (m ~ U[0.01,0.1]), 8-16 shifts log-spaced 1e-4..1 and Gaussian source, all seeded.
+    With shared=True (--config batch-rhs) the 8 systems of a lattice are 8 sources on one gauge field with one mass
+    and shift set (the multi-right-hand-side case: propagators of several sources on one configuration), so the
+    grouped dslash loads each link once for all of them.
     One step = all 24 solved to per-shift true residual 1e-10 by kq_batch_solve (persistent launches over every
     system's tiles, CUDA graphs, autotuned shape); compared with the same 24 solved one after another."""
     import torch
@@ -617,8 +618,11 @@ def run_batch(args, shared=False):
     lattices = [(16, 16, 16, 16)] * 8 + [(24, 24, 24, 48)] * 8 + [(32, 32, 32, 32)] * 8
     systems = []
     field_ctx = {}
+    per_field = {}
     for i, dims in enumerate(lattices):
         eps, mass, ns = rng.uniform(0.2, 0.4), rng.uniform(0.01, 0.1), int(rng.integers(8, 17))
+        if shared:  # one mass and shift set per gauge field
+            eps, mass, ns = per_field.setdefault(dims, (eps, mass, ns))
         V, Vh = int(np.prod(dims)), int(np.prod(dims)) // 2
         if shared and dims in field_ctx:
             ctx = field_ctx[dims]
@@ -681,12 +685,15 @@ def run_batch(args, shared=False):
         "vs_baseline": None, "dtype": "f64+f32" + ("+f16(int16+norm)" if prec == K.KUQCD_HALF else ""),
         "data": "synthetic (seeded on device)",
         "config": {"workload": ("24 systems: 8 x 16^4, 8 x 24^3x48, 8 x 32^4; "
-                                + ("one gauge field per lattice shared by its 8 systems (eps U[0.2,0.4])"
-                                   if shared else "eps U[0.2,0.4], own gauge field each")
-                                + ", m U[0.01,0.1], 8-16 shifts 1e-4..1, per-shift true residual 1e-10"),
+                                + ("8 sources on one gauge field per lattice (eps, m, shift set per field: "
+                                   "eps U[0.2,0.4], m U[0.01,0.1], 8-16 shifts 1e-4..1)"
+                                   if shared else "eps U[0.2,0.4], own gauge field each, m U[0.01,0.1], 8-16 "
+                                                  "shifts 1e-4..1")
+                                + ", per-shift true residual 1e-10"),
                    "solver": "kq_batch_solve (mixed)", "gauge_fields": len(set(id(c) for c, *_ in systems)),
                    "tile": info.tile, "ctas_per_sm": info.ctas_per_sm, "rhs_per_cta": info.rhs_per_cta,
-                   "sites_per_thread": info.sites_per_thread, "groups": info.groups,
+                   "sites_per_thread": info.sites_per_thread, "fp64_rhs_per_pass": info.fp64_rhs_per_pass,
+                   "groups": info.groups,
                    "max_iterations": info.iterations, "refined_systems": info.refined_systems,
                    "refine_iterations": info.refine_iterations,
                    "batched_phase_ms": info.batched_seconds * 1e3, "check_refine_ms": info.check_seconds * 1e3,

@@ -135,15 +135,29 @@ KuQCDStatus kq_slab_pack_faces(kq_context *ctx, int prec, const void *d_src, voi
 size_t kq_slab_link_face_bytes(const kq_context *ctx);               /* FP64 t links, 3 slices, both types */
 KuQCDStatus kq_slab_pack_link_face(kq_context *ctx, void *d_face);  /* top 3 slices, for rank + 1 */
 KuQCDStatus kq_slab_set_link_ghosts(kq_context *ctx, const void *d_face); /* received from rank - 1 */
-/* d_dst (parity dst_parity) = D d_src on the slab, or sigma * d_pvec - D d_src when d_pvec != NULL; DOUBLE or
- * SINGLE.  Replaces DiracHISQ::Dslash with np > 1 (StartComm / interior / EndComm, dirac_hisq.cpp:409-455). */
+/* d_dst (parity dst_parity) = D d_src on the slab, or sigma * d_pvec - D d_src when d_pvec != NULL; DOUBLE,
+ * SINGLE or HALF.  Replaces DiracHISQ::Dslash with np > 1 (StartComm / interior / EndComm, dirac_hisq.cpp:409-455). */
 KuQCDStatus kq_slab_dslash(kq_context *ctx, int prec, const void *d_src, const void *d_ghost_lo,
                            const void *d_ghost_hi, void *d_dst, int dst_parity, const void *d_pvec, double sigma,
                            void *stream);
+/* The dslash of one part of the slab's output sites: part 0 all, 1 the interior (3 <= t < nt_local - 3; reads no
+ * ghost, the ghost pointers may be NULL, so it can run while the faces are in flight), 2 the boundary (the 3 slices at
+ * each end, after the ghosts have arrived).  The interior and boundary launches together equal part 0.  DOUBLE,
+ * SINGLE or HALF (HALF ghost links take the scales of the context's HALF links). */
+KuQCDStatus kq_slab_dslash_part(kq_context *ctx, int prec, const void *d_src, const void *d_ghost_lo,
+                                const void *d_ghost_hi, void *d_dst, int dst_parity, const void *d_pvec, double sigma,
+                                int part, void *stream);
 /* BLAS-1 on FP64 fields of the context (spinor_field.cpp:130-252): y = a x + b y; local Re<x, y> (the caller
  * sums it over ranks, as the reference's MPI_Allreduce does, spinor_field.cpp:207-215) */
 KuQCDStatus kq_field_axpby(kq_context *ctx, double a, const void *d_x, double b, void *d_y, void *stream);
 KuQCDStatus kq_field_dot(kq_context *ctx, const void *d_x, const void *d_y, double *out);
+/* the local Re<x, y> into the device double *d_out, in stream order without a host round trip (an all-reduce over
+ * ranks can then run on the device buffer) */
+KuQCDStatus kq_field_dot_device(kq_context *ctx, const void *d_x, const void *d_y, double *d_out, void *stream);
+/* the shift-vector updates of one CGM iteration (inverter_cgm.cpp:61-69) in one pass: for j < num_shift,
+ * x_j -= B_j p_j, then p_j = Z_j r + a_j p_j; shift j's FP64 fields at d_p + j * stride and d_x + j * stride */
+KuQCDStatus kq_field_ms_update(kq_context *ctx, int num_shift, const double *B, const double *Z, const double *a,
+                               const void *d_r, void *d_p, void *d_x, size_t stride, void *stream);
 
 /* ---------------------------------------------------------------- solver */
 enum {
@@ -224,6 +238,7 @@ typedef struct {
     int tuned_now;            /* 1 when this call measured the launch shape */
     int rhs_per_cta;          /* systems on one gauge field whose dslash shares each link load (1, 2, 4 or 8) */
     int sites_per_thread;     /* sites each thread handles per work item */
+    int fp64_rhs_per_pass;    /* right-hand sides the FP64 dslash serves per link load (1, 2 or 4) */
     int groups;               /* groups of systems sharing link loads (+ systems solved on their own) */
     double check_seconds;     /* wall time of the batched systems' FP64 checks and refinements */
     int refine_iterations;    /* refinement iterations summed over the batched systems */

@@ -107,9 +107,10 @@ __device__ __forceinline__ unsigned group_mask(const GroupDesc &G)
     return use;
 }
 
-// operator-precision members per pass: the FP64 accumulators of more than 4 right-hand sides would not fit the
-// registers next to an FP64 link, so an FP64 group of 8 runs in two passes of 4 (links loaded twice)
-template <int M, int R> struct Pass { static constexpr int v = (M == 0 && R > 4) ? 4 : R; };
+// Members per pass over a tile: every pass loads the links once for its members.  FP64 accumulators take twice the
+// registers, so FP64 passes take at most P64 members (1, 2 or 4, a tuned value): with 4 the FP64 kernel needs ~190
+// registers and one 256-thread CTA per SM, with 1 it keeps the single-system kernel's occupancy and reuses nothing.
+template <int M, int R, int P64> struct Pass { static constexpr int v = M == 0 ? (R < P64 ? R : P64) : R; };
 
 // ---------------------------------------------------------------------------------------------------- kernels
 template <int BS>
@@ -174,19 +175,19 @@ __global__ void __launch_bounds__(BS) bk_init_kernel(const int2 *__restrict__ it
 // Launch bounds of the dslash kernels: one group member (R = 1) keeps the single-system shapes (FP32: three
 // 256-thread CTAs per SM; FP64 and HALF up to 128 registers, at the 85-register cap the long-link row rebuild and
 // the HALF decode spill); several members need room for their accumulators (FP64: one 256-thread CTA per SM).
-template <int BS, int M, int R> struct Bounds {
-    static constexpr int v = R == 1 ? (M == 1 ? 768 : 512) / BS : (M == 0 ? 256 : 512) / BS;
+template <int BS, int M, int RP> struct Bounds {
+    static constexpr int v = RP == 1 ? (M == 1 ? 768 : 512) / BS : (M == 0 ? 256 : 512) / BS;
 };
 
 // K1: tmp_r = D p0_r and |tmp_r|^2 -> beta step with <p0, A p0> = sigma0 |p0|^2 + |tmp|^2 (|p0|^2 from the alpha
 // step's recurrence), for the members of each group whose operator precision is M (one launch per precision, so
 // that each launch is specialised; members in the other precisions are skipped).
-template <int BS, int M, int R>
-__global__ void __launch_bounds__(BS, Bounds<BS, M, R>::v) bk_dslash1_kernel(const int2 *__restrict__ items,
-                                                                            int nitems, int spt)
+template <int BS, int M, int R, int P64>
+__global__ void __launch_bounds__(BS, Bounds<BS, M, Pass<M, R, P64>::v>::v) bk_dslash1_kernel(
+    const int2 *__restrict__ items, int nitems, int spt)
 {
     typedef typename Acc2<M, M>::T T;
-    constexpr int RP = Pass<M, R>::v;
+    constexpr int RP = Pass<M, R, P64>::v;
     __shared__ double sm[32];
 #pragma unroll 1
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
@@ -240,12 +241,12 @@ __global__ void __launch_bounds__(BS, Bounds<BS, M, R>::v) bk_dslash1_kernel(con
 // K2: r_r^(i+1) = r_r^(i) + B0 (sigma0 p0_r - D tmp_r) into each member's ring (s stays in registers), |r_r|^2 ->
 // alpha step, for the members in precision M.  The alpha step picks the next iteration's precision in next_mode,
 // applied in K3, so the K2 launches of the other precisions in this iteration do not pick the system up again.
-template <int BS, int M, int R>
-__global__ void __launch_bounds__(BS, Bounds<BS, M, R>::v) bk_dslash2_kernel(const int2 *__restrict__ items,
-                                                                            int nitems, int spt)
+template <int BS, int M, int R, int P64>
+__global__ void __launch_bounds__(BS, Bounds<BS, M, Pass<M, R, P64>::v>::v) bk_dslash2_kernel(
+    const int2 *__restrict__ items, int nitems, int spt)
 {
     typedef typename Acc2<M, M>::T T;
-    constexpr int RP = Pass<M, R>::v;
+    constexpr int RP = Pass<M, R, P64>::v;
     __shared__ double sm[32];
 #pragma unroll 1
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
@@ -393,29 +394,38 @@ static void enqueue_batch_init(const BatchItems &it, int grid, int spt, cudaStre
     bk_init_kernel<BS><<<grid, BS, 0, s>>>(it.sys, it.nsys, spt);
 }
 
-template <int BS, int R>
+template <int BS, int R, int P64>
 static void enqueue_batch_chunk_r(const BatchItems &it, int grid, int spt, cudaStream_t s)
 {
     for (int k = 0; k < kChunk; ++k) {
-        bk_dslash1_kernel<BS, 0, R><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
-        bk_dslash1_kernel<BS, 1, R><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
-        bk_dslash1_kernel<BS, 2, R><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
-        bk_dslash2_kernel<BS, 0, R><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
-        bk_dslash2_kernel<BS, 1, R><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
-        bk_dslash2_kernel<BS, 2, R><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
+        // (P64 only shapes the FP64 kernels; the sloppy ones are instantiated once)
+        bk_dslash1_kernel<BS, 0, R, P64><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
+        bk_dslash1_kernel<BS, 1, R, 1><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
+        bk_dslash1_kernel<BS, 2, R, 1><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
+        bk_dslash2_kernel<BS, 0, R, P64><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
+        bk_dslash2_kernel<BS, 1, R, 1><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
+        bk_dslash2_kernel<BS, 2, R, 1><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
         bk_p0_kernel<BS><<<grid, BS, 0, s>>>(it.sys, it.nsys, spt);
     }
     bk_window_kernel<BS><<<grid, BS, 0, s>>>(it.sys, it.nsys, spt);
 }
 
+template <int BS, int R>
+static void enqueue_batch_chunk_p(const BatchItems &it, int grid, int spt, int p64, cudaStream_t s)
+{
+    if (R == 1 || p64 == 1) enqueue_batch_chunk_r<BS, R, 1>(it, grid, spt, s);
+    else if (R == 2 || p64 == 2) enqueue_batch_chunk_r<BS, R, 2>(it, grid, spt, s);
+    else enqueue_batch_chunk_r<BS, R, 4>(it, grid, spt, s);
+}
+
 template <int BS>
-static void enqueue_batch_chunk(const BatchItems &it, int grid, int rhs, int spt, cudaStream_t s)
+static void enqueue_batch_chunk(const BatchItems &it, int grid, int rhs, int spt, int p64, cudaStream_t s)
 {
     switch (rhs) {
-        case 8: enqueue_batch_chunk_r<BS, 8>(it, grid, spt, s); break;
-        case 4: enqueue_batch_chunk_r<BS, 4>(it, grid, spt, s); break;
-        case 2: enqueue_batch_chunk_r<BS, 2>(it, grid, spt, s); break;
-        default: enqueue_batch_chunk_r<BS, 1>(it, grid, spt, s); break;
+        case 8: enqueue_batch_chunk_p<BS, 8>(it, grid, spt, p64, s); break;
+        case 4: enqueue_batch_chunk_p<BS, 4>(it, grid, spt, p64, s); break;
+        case 2: enqueue_batch_chunk_p<BS, 2>(it, grid, spt, p64, s); break;
+        default: enqueue_batch_chunk_r<BS, 1, 1>(it, grid, spt, s); break;
     }
 }
 
@@ -659,7 +669,7 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
     const int shared = max_shared(b->sys);
 
     // launch shape: tuned once per batch signature (sizes, shared gauge fields, shifts, schedule), cached on disk
-    std::string key = "batch2";
+    std::string key = "batch3";
     for (auto &S : b->sys) {
         int owner = 0;  // first system on the same context: systems sharing links share this number
         while (b->sys[owner].ctx != S.ctx) ++owner;
@@ -670,12 +680,14 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
     }
     BatchTune tune;
     bool have_tune = tune_lookup(key, &tune);
-    // KUQCD_BATCH_SHAPE="threads,ctas_per_sm,rhs,sites_per_thread" fixes the shape (no tuning, no cache)
+    // KUQCD_BATCH_SHAPE="threads,ctas_per_sm,rhs,sites_per_thread[,fp64_rhs_per_pass]" fixes the shape (no tuning)
     if (const char *shape = getenv("KUQCD_BATCH_SHAPE")) {
-        BatchTune t{256, 4, 1, 1};
-        if (sscanf(shape, "%d,%d,%d,%d", &t.bs, &t.ctas_per_sm, &t.rhs, &t.spt) == 4 && (t.bs == 128 || t.bs == 256) &&
-            t.ctas_per_sm >= 1 && t.ctas_per_sm <= 32 && (t.rhs == 1 || t.rhs == 2 || t.rhs == 4 || t.rhs == 8) &&
-            (t.spt == 1 || t.spt == 2)) {
+        BatchTune t{256, 4, 1, 1, 1};
+        const int n = sscanf(shape, "%d,%d,%d,%d,%d", &t.bs, &t.ctas_per_sm, &t.rhs, &t.spt, &t.p64);
+        if (n == 4) t.p64 = t.rhs < 4 ? t.rhs : 4;
+        if (n >= 4 && (t.bs == 128 || t.bs == 256) && t.ctas_per_sm >= 1 && t.ctas_per_sm <= 32 &&
+            (t.rhs == 1 || t.rhs == 2 || t.rhs == 4 || t.rhs == 8) && (t.spt == 1 || t.spt == 2) &&
+            (t.p64 == 1 || t.p64 == 2 || t.p64 == 4)) {
             tune = t;
             have_tune = true;
         }
@@ -685,6 +697,7 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
         tune.ctas_per_sm = 4;
         tune.rhs = 1;
         tune.spt = 1;
+        tune.p64 = 1;
     }
 
     auto run = [&](const BatchTune &t, int max_chunks, float *ms_out, long long *launches, int *chunks_out,
@@ -732,8 +745,8 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         KQ_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        if (t.bs == 128) enqueue_batch_chunk<128>(items, grid, t.rhs, t.spt, s);
-        else enqueue_batch_chunk<256>(items, grid, t.rhs, t.spt, s);
+        if (t.bs == 128) enqueue_batch_chunk<128>(items, grid, t.rhs, t.spt, t.p64, s);
+        else enqueue_batch_chunk<256>(items, grid, t.rhs, t.spt, t.p64, s);
         cudaError_t ee = cudaStreamEndCapture(s, &graph);
         if (ee == cudaSuccess) ee = cudaGraphInstantiate(&exec, graph, 0);
         if (graph) cudaGraphDestroy(graph);
@@ -782,7 +795,7 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
         };
         int rmax = 1;
         while (rmax < std::min(shared, kMaxR)) rmax *= 2;
-        BatchTune t{256, 4, rmax, 1};
+        BatchTune t{256, 4, rmax, 1, std::min(rmax, 4)};
         const int bss[2] = {128, 256}, cpss[4] = {2, 4, 8, 16};
         for (int bs : bss)
             for (int cps : cpss) {
@@ -797,6 +810,16 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
             if (r == t.rhs) continue;
             BatchTune c = t;
             c.rhs = r;
+            c.p64 = std::min(r, 4);
+            const cudaError_t e = trial(c);
+            if (e != cudaSuccess) return status_of(e);
+        }
+        // FP64 right-hand sides per pass, below the full group: occupancy against link reuse in the FP64 phase (the
+        // timed windows are the solve's first, which run on FP64 links)
+        t = tune;
+        for (int p = 1; p < std::min(t.rhs, 4); p *= 2) {
+            BatchTune c = t;
+            c.p64 = p;
             const cudaError_t e = trial(c);
             if (e != cudaSuccess) return status_of(e);
         }
@@ -908,6 +931,7 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
         out->tuned_now = have_tune ? 0 : 1;
         out->rhs_per_cta = tune.rhs;
         out->sites_per_thread = tune.spt;
+        out->fp64_rhs_per_pass = tune.p64;
         out->groups = ngroups;
         out->check_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_check).count();
         out->refine_iterations = refine_total;
@@ -1003,6 +1027,7 @@ KQ_API KuQCDStatus kq_batch_solve(kq_batch *b, kq_batch_info *out)
         out->tuned_now = bi.tuned_now;
         out->rhs_per_cta = bi.rhs_per_cta;
         out->sites_per_thread = bi.sites_per_thread;
+        out->fp64_rhs_per_pass = bi.fp64_rhs_per_pass;
         out->groups = bi.groups + (int)large.size();
         out->check_seconds = bi.check_seconds;
         out->refine_iterations = bi.refine_iterations;

@@ -226,7 +226,8 @@ KQ_API KuQCDStatus kq_load_links(kq_context *ctx, int link_type, const void *hos
     }
     if (link_type == KUQCD_FAT_LINK) ctx->fat_loaded = true;
     else ctx->long_loaded = true;
-    ctx->have_ghost[0] = ctx->have_ghost[1] = false;  // a slab's ghost links belong to the previous links
+    ctx->have_ghost[0] = ctx->have_ghost[1] = ctx->have_ghost[2] = false;  // a slab's ghost links belong to the
+                                                                           // previous links
     if (link_type == KUQCD_LONG_LINK) {
         e = compress_long(ctx, mp);
         if (e != cudaSuccess) {

@@ -21,10 +21,10 @@ struct kq_context {
     kq::CgmPoll *poll = nullptr;  // pinned host page for state polling
     // t-slab of a domain-decomposed lattice (kq_slab.cu): this context holds local t = 0 .. nt-1 of global
     // t0 = slab_rank * nt; ghost links are the t-direction fat and long links of the 3 slices below t0, per
-    // precision (P64, P32): [fat par0 | fat par1 | long par0 | long par1], each one direction of 3 slices
+    // precision (P64, P32, P16): [fat par0 | fat par1 | long par0 | long par1], each one direction of 3 slices
     int slab_rank = -1, slab_nranks = 0;
-    void *ghost_links[2] = {nullptr, nullptr};
-    bool have_ghost[2] = {false, false};
+    void *ghost_links[3] = {nullptr, nullptr, nullptr};  // per precision: P64 (received), P32, P16 (derived)
+    bool have_ghost[3] = {false, false, false};
     // Solution notification of a parity solve (set by kq_solve_multishift for the duration of one call): the
     // solvers call solution_ready(ctx, k, user) on the host thread once solution k of their d_x holds the value it
     // will be returned with, and again if a later phase changes it.  Work it enqueues on `stream` runs after

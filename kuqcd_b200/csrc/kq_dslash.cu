@@ -3,6 +3,7 @@
 // streamed from HBM once, neighbour spinors come through L1/L2.  Link and spinor precisions are independent
 // template parameters (FP64/FP64, FP32/FP32, HALF/HALF, HALF links with FP32 spinors).
 #include <cstdlib>
+#include <cstring>
 
 #include "kq_dslash_core.cuh"
 #include "kq_dslash_half2.cuh"
@@ -62,14 +63,17 @@ __global__ void __launch_bounds__(256) dslash_full_kernel(Geom g, int pv, LinkSe
     st_spinor<SP>(dst + p * half, pv, i, acc);
 }
 
-// KUQCD_HALF_DSLASH=site selects the one-site-per-thread HALF kernel instead of the two-site packed one
-static bool half_pairs()
+// HALF kernel: 0 one site per thread, 4 / 5 two sites per thread in packed FP32 with 4 / 5 resident 128-thread
+// CTAs per SM (KUQCD_HALF_DSLASH = site | pair4 | pair5; default pair5)
+static int half_kernel()
 {
-    static const bool pairs = [] {
+    static const int k = [] {
         const char *e = getenv("KUQCD_HALF_DSLASH");
-        return !(e && e[0] == 's');
+        if (!e) return 5;
+        if (e[0] == 's') return 0;
+        return strcmp(e, "pair4") == 0 ? 4 : 5;
     }();
-    return pairs;
+    return k;
 }
 
 static bool pair_ok(int lp, int sp)
@@ -91,11 +95,14 @@ cudaError_t launch_dslash2(const Geom &g, const GaugeDev &gd, int lp, int sp, co
         return cudaErrorInvalidValue;
     }
     const int pv = pad_sites(g.vh);
-    if (lp == P16 && sp == P16 && !gate && half_pairs()) {
+    if (lp == P16 && sp == P16 && !gate && half_kernel() != 0) {
         // HALF: two sites per thread in packed FP32 (kq_dslash_half2.cuh)
         constexpr int kBS2 = 128;
         const int nb2 = (g.vh + 2 * kBS2 - 1) / (2 * kBS2);
-        dslash_half2_kernel<kBS2><<<nb2, kBS2, 0, s>>>(g, pv, gd.fat[lp], gd.lng[lp], src, dst, dst_parity);
+        if (half_kernel() == 4)
+            dslash_half2_kernel<kBS2, 4><<<nb2, kBS2, 0, s>>>(g, pv, gd.fat[lp], gd.lng[lp], src, dst, dst_parity);
+        else
+            dslash_half2_kernel<kBS2, 5><<<nb2, kBS2, 0, s>>>(g, pv, gd.fat[lp], gd.lng[lp], src, dst, dst_parity);
         return cudaGetLastError();
     }
     const int bs = block > 0 ? block : 256;

@@ -5,8 +5,8 @@
 // issue competes with its memory time.  Here every thread computes the sites i and i + BS of its block: the two
 // sites' values sit side by side in 64-bit register pairs and one f32x2 instruction does the work of two FP32 ones
 // (mat-vec FMAs, the int16 bias subtraction, the spinor norm products).  The arithmetic per site is that of the
-// one-site kernel (dslash_site2<2,2>: the same int16 decode, the per-field link scales folded out, FP32 sums), so
-// both give the same values up to the order of the backward-hop subtraction.
+// one-site kernel (dslash_site2<2,2>: the same int16 decode, the per-field link scales folded out, FP32 sums); the
+// backward hops enter with their spinor negated in the decode, so one accumulator serves all sixteen terms.
 #pragma once
 #include "kq_dslash_core.cuh"
 
@@ -91,10 +91,11 @@ __device__ __forceinline__ void ld_link_pair(const void *par_base, int pv, int d
     u[17] = q_hi(w0, w1);
 }
 
-// HALF spinors of sites n0, n1: v = q * norm / 32767 (times an extra factor, the long-link scale ratio); nv: the
-// component that enters the mat-vec with a minus sign (imaginary parts for U v, real parts for U^dag v)
+// HALF spinors of sites n0, n1: v = q * norm / 32767 times `extra` (the long-link scale ratio; negative for the
+// backward hops, whose terms are subtracted); w: the three components that enter the mat-vec with the other sign
+// (-imaginary parts for U v, -real parts for U^dag v)
 template <bool ADJ>
-__device__ __forceinline__ void ld_spinor_pair(const void *base, int n0, int n1, f2 extra, f2 v[6], f2 nv[3])
+__device__ __forceinline__ void ld_spinor_pair(const void *base, int n0, int n1, f2 extra, f2 v[6], f2 w[3])
 {
     const int4 a = __ldg(static_cast<const int4 *>(base) + n0), b = __ldg(static_cast<const int4 *>(base) + n1);
     const f2 s = mul2(pack(__int_as_float(a.w), __int_as_float(b.w)), extra);
@@ -103,11 +104,11 @@ __device__ __forceinline__ void ld_spinor_pair(const void *base, int n0, int n1,
     v[4] = mul2(q_lo(a.z, b.z), s); v[5] = mul2(q_hi(a.z, b.z), s);
     const f2 m1 = pack(-1.f, -1.f);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) nv[c] = mul2(v[2 * c + (ADJ ? 0 : 1)], m1);
+    for (int c = 0; c < 3; ++c) w[c] = mul2(v[2 * c + (ADJ ? 0 : 1)], m1);
 }
 
-// acc += U v   (re += ur vr - ui vi, im += ur vi + ui vr)
-__device__ __forceinline__ void mv_add2(const f2 u[18], const f2 v[6], const f2 nvi[3], f2 acc[6])
+// acc += U v   (re += ur vr - ui vi, im += ur vi + ui vr); w = -vi
+__device__ __forceinline__ void mv_add2(const f2 u[18], const f2 v[6], const f2 w[3], f2 acc[6])
 {
 #pragma unroll
     for (int r = 0; r < 3; ++r)
@@ -115,14 +116,15 @@ __device__ __forceinline__ void mv_add2(const f2 u[18], const f2 v[6], const f2 
         for (int c = 0; c < 3; ++c) {
             const f2 ur = u[2 * (c + 3 * r)], ui = u[2 * (c + 3 * r) + 1];
             acc[2 * r] = fma2(ur, v[2 * c], acc[2 * r]);
-            acc[2 * r] = fma2(ui, nvi[c], acc[2 * r]);
+            acc[2 * r] = fma2(ui, w[c], acc[2 * r]);
             acc[2 * r + 1] = fma2(ur, v[2 * c + 1], acc[2 * r + 1]);
             acc[2 * r + 1] = fma2(ui, v[2 * c], acc[2 * r + 1]);
         }
 }
 
-// acc += U^dag v   ((U^dag v)_r = sum_c conj(U_cr) v_c: re += ur vr + ui vi, im += ur vi - ui vr)
-__device__ __forceinline__ void mdv_add2(const f2 u[18], const f2 v[6], const f2 nvr[3], f2 acc[6])
+// acc += U^dag v   ((U^dag v)_r = sum_c conj(U_cr) v_c: re += ur vr + ui vi, im += ur vi - ui vr); w = -vr.
+// The backward hops come with v already negated, so this adds -U^dag v_true into the one accumulator.
+__device__ __forceinline__ void mdv_add2(const f2 u[18], const f2 v[6], const f2 w[3], f2 acc[6])
 {
 #pragma unroll
     for (int r = 0; r < 3; ++r)
@@ -132,7 +134,7 @@ __device__ __forceinline__ void mdv_add2(const f2 u[18], const f2 v[6], const f2
             acc[2 * r] = fma2(ur, v[2 * c], acc[2 * r]);
             acc[2 * r] = fma2(ui, v[2 * c + 1], acc[2 * r]);
             acc[2 * r + 1] = fma2(ur, v[2 * c + 1], acc[2 * r + 1]);
-            acc[2 * r + 1] = fma2(ui, nvr[c], acc[2 * r + 1]);
+            acc[2 * r + 1] = fma2(ui, w[c], acc[2 * r + 1]);
         }
 }
 
@@ -140,8 +142,8 @@ __device__ __forceinline__ void mdv_add2(const f2 u[18], const f2 v[6], const f2
 
 // dst = D src on HALF fields, sites i0 = block * 2 BS + t and i1 = i0 + BS (i1 past the end: computed on i0's
 // neighbours and not stored)
-template <int BS>
-__global__ void __launch_bounds__(BS, 4) dslash_half2_kernel(Geom g, int pv, LinkSet fat, LinkSet lng,
+template <int BS, int MINB>
+__global__ void __launch_bounds__(BS, MINB) dslash_half2_kernel(Geom g, int pv, LinkSet fat, LinkSet lng,
                                                           const void *__restrict__ src, void *__restrict__ dst, int p)
 {
     using namespace h2;
@@ -157,32 +159,33 @@ __global__ void __launch_bounds__(BS, 4) dslash_half2_kernel(Geom g, int pv, Lin
     // (the link values stay raw int16 and the fat scale is applied once at the end)
     const float inv = 1.0f / 32767.0f, rl = lng.scale / fat.scale;
     const f2 e_fat = pack(inv, inv), e_lng = pack(inv * rl, inv * rl);
-    f2 accf[6], accb[6];
+    const f2 n_fat = pack(-inv, -inv), n_lng = pack(-inv * rl, -inv * rl);  // backward hops: subtracted
+    f2 acc[6];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) accf[k] = accb[k] = pack(0.f, 0.f);
+    for (int k = 0; k < 6; ++k) acc[k] = pack(0.f, 0.f);
 #pragma unroll
     for (int dir = 0; dir < 4; ++dir) {
-        f2 u[18], v[6], nv[3];
+        f2 u[18], v[6], w[3];
         ld_link_pair(fat_p, pv, dir, i0, i1, u);
-        ld_spinor_pair<false>(src, nbr_index(g, c0, i0, dir, 1), nbr_index(g, c1, i1, dir, 1), e_fat, v, nv);
-        mv_add2(u, v, nv, accf);
+        ld_spinor_pair<false>(src, nbr_index(g, c0, i0, dir, 1), nbr_index(g, c1, i1, dir, 1), e_fat, v, w);
+        mv_add2(u, v, w, acc);
         ld_link_pair(lng_p, pv, dir, i0, i1, u);
-        ld_spinor_pair<false>(src, nbr_index(g, c0, i0, dir, 3), nbr_index(g, c1, i1, dir, 3), e_lng, v, nv);
-        mv_add2(u, v, nv, accf);
+        ld_spinor_pair<false>(src, nbr_index(g, c0, i0, dir, 3), nbr_index(g, c1, i1, dir, 3), e_lng, v, w);
+        mv_add2(u, v, w, acc);
         const int b10 = nbr_index(g, c0, i0, dir, -1), b11 = nbr_index(g, c1, i1, dir, -1);
         ld_link_pair(fat_q, pv, dir, b10, b11, u);
-        ld_spinor_pair<true>(src, b10, b11, e_fat, v, nv);
-        mdv_add2(u, v, nv, accb);
+        ld_spinor_pair<true>(src, b10, b11, n_fat, v, w);
+        mdv_add2(u, v, w, acc);
         const int b30 = nbr_index(g, c0, i0, dir, -3), b31 = nbr_index(g, c1, i1, dir, -3);
         ld_link_pair(lng_q, pv, dir, b30, b31, u);
-        ld_spinor_pair<true>(src, b30, b31, e_lng, v, nv);
-        mdv_add2(u, v, nv, accb);
+        ld_spinor_pair<true>(src, b30, b31, n_lng, v, w);
+        mdv_add2(u, v, w, acc);
     }
     const float sf = fat.scale * inv;
     const f2 s2 = pack(sf, sf);
     float o0[6], o1[6];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) unpack(mul2(sub2(accf[k], accb[k]), s2), o0[k], o1[k]);
+    for (int k = 0; k < 6; ++k) unpack(mul2(acc[k], s2), o0[k], o1[k]);
     st_spinor<2>(dst, pv, i0, o0);
     if (two) st_spinor<2>(dst, pv, i1, o1);
 }

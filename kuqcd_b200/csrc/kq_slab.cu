@@ -20,6 +20,7 @@
 
 #include "kq_context.h"
 #include "kq_dslash_core.cuh"
+#include "kq_msrelax.h"
 
 namespace kq {
 
@@ -86,7 +87,9 @@ __device__ __forceinline__ void slab_site(const Geom &g, int pv, const LinkSet &
                     else ld_link_any<P>(lng_q, pv, 3, i - h * S, lng.scale, lng.recon, u);
                     ld_spinor<P>(src, pv, i - h * S, v);
                 } else {
-                    ld_link<P>(h == 1 ? a.gfat_q : a.glng_q, a.pvg, 0, (tt + 3) * S + j, 1.f, u);
+                    // ghost links share the local fields' HALF scales (unused in FP64 / FP32)
+                    ld_link<P>(h == 1 ? a.gfat_q : a.glng_q, a.pvg, 0, (tt + 3) * S + j,
+                               h == 1 ? fat.scale : lng.scale, u);
                     ld_spinor<P>(a.glo, a.pvg, (tt + 3) * S + j, v);
                 }
                 mdv_sub(u, v, acc);
@@ -95,14 +98,36 @@ __device__ __forceinline__ void slab_site(const Geom &g, int pv, const LinkSet &
     }
 }
 
+// Which output sites a launch covers.  Interior sites (3 <= t < nt_local - 3) read no ghost, so their dslash can
+// run while the faces are in flight; the boundary sites (the 3 slices at each end) wait for the ghosts.
+enum { kSlabAll = 0, kSlabInterior = 1, kSlabBoundary = 2 };
+
+__host__ __device__ inline int slab_part_sites(const Geom &g, int part)
+{
+    const int S = g.st, lt = g.n[3];
+    if (part == kSlabInterior) return lt > 6 ? (lt - 6) * S : 0;
+    if (part == kSlabBoundary) return lt > 6 ? 6 * S : g.vh;
+    return g.vh;
+}
+
+// site of entry k of a part
+__device__ __forceinline__ int slab_part_site(const Geom &g, int part, int k)
+{
+    const int S = g.st, lt = g.n[3];
+    if (part == kSlabInterior) return 3 * S + k;
+    if (part == kSlabBoundary && lt > 6) return k < 3 * S ? k : k + (lt - 6) * S;
+    return k;
+}
+
 template <int P>
 __global__ void __launch_bounds__(256) slab_dslash_kernel(Geom g, int pv, LinkSet fat, LinkSet lng,
                                                           const void *__restrict__ src, SlabArgs a,
-                                                          void *__restrict__ dst, int p)
+                                                          void *__restrict__ dst, int p, int part)
 {
     using T = typename Acc2<P, P>::T;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.vh) return;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= slab_part_sites(g, part)) return;
+    const int i = slab_part_site(g, part, k);
     T acc[6];
     slab_site<P>(g, pv, fat, lng, src, a, p, i, acc);
     if (a.pvec) {
@@ -146,9 +171,11 @@ __global__ void slab_link_pack_kernel(Geom g, int pv, LinkSet fat, LinkSet lng, 
     }
 }
 
-// FP64 ghost links -> FP32 copy
-__global__ void slab_link_to32_kernel(int n, int pvg, size_t part64, const char *__restrict__ g64, size_t part32,
-                                      char *__restrict__ g32)
+// FP64 ghost links -> FP32 copy, or a HALF copy with the per-field scales of the local HALF links (fat for the
+// two fat parts, long for the two long parts) and the same device factors
+template <int P>
+__global__ void slab_link_conv_kernel(int n, int pvg, size_t part64, const char *__restrict__ g64, size_t partp,
+                                      char *__restrict__ gp, float scale_fat, float scale_lng)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -156,7 +183,49 @@ __global__ void slab_link_to32_kernel(int n, int pvg, size_t part64, const char 
     for (int q = 0; q < 4; ++q) {
         double u[18];
         ld_link<0>(g64 + q * part64, pvg, 0, k, 1.f, u);
-        st_link<1>(g32 + q * part32, pvg, 0, k, 1.f, u);
+        if (P == 2) {
+            // the local field's scale need not cover a neighbour's largest entry: saturate instead of wrapping
+            const double lim = (double)(q < 2 ? scale_fat : scale_lng);
+#pragma unroll
+            for (int e = 0; e < 18; ++e) u[e] = fmin(fmax(u[e], -lim), lim);
+        }
+        st_link<P>(gp + q * partp, pvg, 0, k, q < 2 ? scale_fat : scale_lng, u);
+    }
+}
+
+// <x, y> of FP64 fields summed into *out on the device: block partials, then one block over them in a fixed order
+__global__ void field_sum_kernel(const double *__restrict__ partials, int n, double *__restrict__ out)
+{
+    __shared__ double sm[32];
+    double s = 0.0;
+    for (int b = threadIdx.x; b < n; b += blockDim.x) s += partials[b];
+    s = block_sum(s, sm);
+    if (threadIdx.x == 0) *out = s;
+}
+
+// the shift vectors of one multishift CG iteration (inverter_cgm.cpp:61-69): x_j -= B_j p_j, then
+// p_j = Z_j r + a_j p_j, for j < nshift; shift j's fields at base + j * stride
+struct MsCoef {
+    double B[kMaxShift], Z[kMaxShift], a[kMaxShift];
+};
+__global__ void field_ms_update_kernel(int vh, int pv, int nshift, MsCoef c, const void *__restrict__ r, char *p,
+                                       char *x, size_t stride)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= vh) return;
+    double rv[6];
+    ld_spinor<0>(r, pv, i, rv);
+    for (int j = 0; j < nshift; ++j) {
+        double pv6[6], xv[6];
+        ld_spinor<0>(p + j * stride, pv, i, pv6);
+        ld_spinor<0>(x + j * stride, pv, i, xv);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            xv[k] -= c.B[j] * pv6[k];
+            pv6[k] = c.Z[j] * rv[k] + c.a[j] * pv6[k];
+        }
+        st_spinor<0>(x + j * stride, pv, i, xv);
+        st_spinor<0>(p + j * stride, pv, i, pv6);
     }
 }
 
@@ -195,7 +264,7 @@ static int face_pitch(const Geom &g) { return pad_sites(face_sites(g)); }
 
 static size_t ghost_link_part(const Geom &g, int prec)  // one type, one parity, one direction, 3 slices
 {
-    return (size_t)(prec == P64 ? 144 : 72) * face_pitch(g);
+    return (size_t)(prec == P64 ? 144 : prec == P32 ? 72 : 36) * face_pitch(g);
 }
 
 }  // namespace kq
@@ -224,7 +293,7 @@ KQ_API KuQCDStatus kq_slab_set(kq_context *ctx, int rank, int nranks)
     }
     ctx->slab_rank = rank;
     ctx->slab_nranks = nranks;
-    ctx->have_ghost[0] = ctx->have_ghost[1] = false;
+    ctx->have_ghost[0] = ctx->have_ghost[1] = ctx->have_ghost[2] = false;
     return KUQCD_SUCCESS;
 }
 
@@ -293,34 +362,43 @@ KQ_API KuQCDStatus kq_slab_set_link_ghosts(kq_context *ctx, const void *d_face)
     if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->ghost_links[0], d_face, bytes, cudaMemcpyDeviceToDevice, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     ctx->have_ghost[0] = e == cudaSuccess;
-    ctx->have_ghost[1] = false;
+    ctx->have_ghost[1] = ctx->have_ghost[2] = false;
     return status_of(e);
 }
 
-static cudaError_t ensure_ghost32(kq_context *ctx)
+// ghost links in a sloppy precision, derived once from the FP64 ghosts (HALF with the local HALF links' scales)
+static cudaError_t ensure_ghost(kq_context *ctx, int p)
 {
-    if (ctx->have_ghost[1]) return cudaSuccess;
+    if (p == P64 || ctx->have_ghost[p]) return cudaSuccess;
     const Geom &g = ctx->g;
-    if (!ctx->ghost_links[1]) KQ_CUDA_TRY(cudaMalloc(&ctx->ghost_links[1], 4 * ghost_link_part(g, P32)));
-    const int n = face_sites(g);
-    slab_link_to32_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(
-        n, face_pitch(g), ghost_link_part(g, P64), static_cast<const char *>(ctx->ghost_links[0]),
-        ghost_link_part(g, P32), static_cast<char *>(ctx->ghost_links[1]));
+    if (!ctx->ghost_links[p]) KQ_CUDA_TRY(cudaMalloc(&ctx->ghost_links[p], 4 * ghost_link_part(g, p)));
+    const int n = face_sites(g), nb = (n + 255) / 256;
+    const char *g64 = static_cast<const char *>(ctx->ghost_links[0]);
+    char *gp = static_cast<char *>(ctx->ghost_links[p]);
+    if (p == P32)
+        slab_link_conv_kernel<1><<<nb, 256, 0, ctx->stream>>>(n, face_pitch(g), ghost_link_part(g, P64), g64,
+                                                              ghost_link_part(g, P32), gp, 1.f, 1.f);
+    else
+        slab_link_conv_kernel<2><<<nb, 256, 0, ctx->stream>>>(n, face_pitch(g), ghost_link_part(g, P64), g64,
+                                                              ghost_link_part(g, P16), gp, ctx->gd.fat[P16].scale,
+                                                              ctx->gd.lng[P16].scale);
     KQ_CUDA_TRY(cudaGetLastError());
-    ctx->have_ghost[1] = true;
+    ctx->have_ghost[p] = true;
     return cudaSuccess;
 }
 
-KQ_API KuQCDStatus kq_slab_dslash(kq_context *ctx, int prec, const void *d_src, const void *d_ghost_lo,
-                                  const void *d_ghost_hi, void *d_dst, int dst_parity, const void *d_pvec,
-                                  double sigma, void *stream)
+KQ_API KuQCDStatus kq_slab_dslash_part(kq_context *ctx, int prec, const void *d_src, const void *d_ghost_lo,
+                                       const void *d_ghost_hi, void *d_dst, int dst_parity, const void *d_pvec,
+                                       double sigma, int part, void *stream)
 {
     KuQCDStatus st = slab_check(ctx, "kq_slab_dslash");
     if (st != KUQCD_SUCCESS) return st;
-    if (!d_src || !d_ghost_lo || !d_ghost_hi || !d_dst) return KUQCD_ERR_NULL_POINTER;
+    if (part != kSlabAll && part != kSlabInterior && part != kSlabBoundary) return KUQCD_ERR_INVALID_PARAM;
+    // the interior reads no ghost: its launch may run before the ghosts exist
+    if (!d_src || !d_dst || (part != kSlabInterior && (!d_ghost_lo || !d_ghost_hi))) return KUQCD_ERR_NULL_POINTER;
     const int p = prec_from_api(prec);
-    if ((p != P64 && p != P32) || (dst_parity != 0 && dst_parity != 1)) {
-        set_last_error("kq_slab_dslash: DOUBLE or SINGLE, parity 0 or 1");
+    if (p < 0 || (dst_parity != 0 && dst_parity != 1)) {
+        set_last_error("kq_slab_dslash: DOUBLE, SINGLE or HALF, parity 0 or 1");
         return KUQCD_ERR_INVALID_PARAM;
     }
     if (!ctx->have_ghost[0]) {
@@ -332,26 +410,85 @@ KQ_API KuQCDStatus kq_slab_dslash(kq_context *ctx, int prec, const void *d_src, 
         if (st != KUQCD_SUCCESS) return st;
     }
     cudaSetDevice(ctx->device);
-    cudaError_t e = p == P32 ? ensure_ghost32(ctx) : cudaSuccess;
+    cudaError_t e = ensure_ghost(ctx, p);
     if (e != cudaSuccess) return status_of(e);
     const Geom &g = ctx->g;
-    const size_t part = ghost_link_part(g, p);
+    const size_t gpart = ghost_link_part(g, p);
     const char *gl = static_cast<const char *>(ctx->ghost_links[p]);
     const int q = 1 - dst_parity;
     SlabArgs a;
     a.glo = d_ghost_lo;
     a.ghi = d_ghost_hi;
     a.pvg = face_pitch(g);
-    a.gfat_q = gl + (0 + q) * part;
-    a.glng_q = gl + (2 + q) * part;
+    a.gfat_q = gl + (0 + q) * gpart;
+    a.glng_q = gl + (2 + q) * gpart;
     a.pvec = d_pvec;
     a.sigma = sigma;
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
-    const int nb = (g.vh + 255) / 256, pv = pad_sites(g.vh);
-    if (p == P64)
-        slab_dslash_kernel<0><<<nb, 256, 0, s>>>(g, pv, ctx->gd.fat[P64], ctx->gd.lng[P64], d_src, a, d_dst, dst_parity);
-    else
-        slab_dslash_kernel<1><<<nb, 256, 0, s>>>(g, pv, ctx->gd.fat[P32], ctx->gd.lng[P32], d_src, a, d_dst, dst_parity);
+    if (stream && stream != (void *)ctx->stream) {
+        // the sloppy ghost links were derived on the context's stream
+        cudaEvent_t ev;
+        e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) return status_of(e);
+        cudaEventRecord(ev, ctx->stream);
+        cudaStreamWaitEvent(s, ev, 0);
+        cudaEventDestroy(ev);
+    }
+    const int n = slab_part_sites(g, part);
+    if (n == 0) return KUQCD_SUCCESS;
+    const int nb = (n + 255) / 256, pv = pad_sites(g.vh);
+    const LinkSet &F = ctx->gd.fat[p], &Lk = ctx->gd.lng[p];
+    if (p == P64) slab_dslash_kernel<0><<<nb, 256, 0, s>>>(g, pv, F, Lk, d_src, a, d_dst, dst_parity, part);
+    else if (p == P32) slab_dslash_kernel<1><<<nb, 256, 0, s>>>(g, pv, F, Lk, d_src, a, d_dst, dst_parity, part);
+    else slab_dslash_kernel<2><<<nb, 256, 0, s>>>(g, pv, F, Lk, d_src, a, d_dst, dst_parity, part);
+    return status_of(cudaGetLastError());
+}
+
+KQ_API KuQCDStatus kq_slab_dslash(kq_context *ctx, int prec, const void *d_src, const void *d_ghost_lo,
+                                  const void *d_ghost_hi, void *d_dst, int dst_parity, const void *d_pvec,
+                                  double sigma, void *stream)
+{
+    return kq_slab_dslash_part(ctx, prec, d_src, d_ghost_lo, d_ghost_hi, d_dst, dst_parity, d_pvec, sigma, kSlabAll,
+                               stream);
+}
+
+KQ_API KuQCDStatus kq_field_dot_device(kq_context *ctx, const void *d_x, const void *d_y, double *d_out,
+                                       void *stream)
+{
+    if (!ctx || !d_x || !d_y || !d_out) return KUQCD_ERR_NULL_POINTER;
+    cudaSetDevice(ctx->device);
+    const Geom &g = ctx->g;
+    const int nb = (g.vh + 255) / 256;
+    Carve probe(nullptr);
+    probe.take(sizeof(double) * nb);
+    cudaError_t e = ensure_work(ctx, probe.off);
+    if (e != cudaSuccess) return status_of(e);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    double *partials = static_cast<double *>(ctx->work);
+    field_dot_kernel<<<nb, 256, 0, s>>>(g.vh, pad_sites(g.vh), d_x, d_y, partials);
+    field_sum_kernel<<<1, 256, 0, s>>>(partials, nb, d_out);
+    return status_of(cudaGetLastError());
+}
+
+KQ_API KuQCDStatus kq_field_ms_update(kq_context *ctx, int num_shift, const double *B, const double *Z,
+                                      const double *a, const void *d_r, void *d_p, void *d_x, size_t stride,
+                                      void *stream)
+{
+    if (!ctx || !B || !Z || !a || !d_r || !d_p || !d_x) return KUQCD_ERR_NULL_POINTER;
+    if (num_shift < 0 || num_shift > kMaxShift) return KUQCD_ERR_INVALID_PARAM;
+    if (num_shift == 0) return KUQCD_SUCCESS;
+    cudaSetDevice(ctx->device);
+    MsCoef c;
+    for (int j = 0; j < num_shift; ++j) {
+        c.B[j] = B[j];
+        c.Z[j] = Z[j];
+        c.a[j] = a[j];
+    }
+    const Geom &g = ctx->g;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    field_ms_update_kernel<<<(g.vh + 255) / 256, 256, 0, s>>>(g.vh, pad_sites(g.vh), num_shift, c, d_r,
+                                                              static_cast<char *>(d_p), static_cast<char *>(d_x),
+                                                              stride);
     return status_of(cudaGetLastError());
 }
 

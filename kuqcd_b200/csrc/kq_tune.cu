@@ -79,7 +79,8 @@ bool tune_lookup(const std::string &key, BatchTune *out)
     if (it == g_cache.end()) return false;
     std::istringstream is(it->second);
     BatchTune t;
-    if (!(is >> t.bs >> t.ctas_per_sm >> t.rhs >> t.spt)) return false;
+    if (!(is >> t.bs >> t.ctas_per_sm >> t.rhs >> t.spt >> t.p64)) return false;
+    if (t.p64 != 1 && t.p64 != 2 && t.p64 != 4) return false;
     if (t.bs != 128 && t.bs != 256) return false;
     if (t.ctas_per_sm < 1 || t.ctas_per_sm > 32) return false;
     if (t.rhs != 1 && t.rhs != 2 && t.rhs != 4 && t.rhs != 8) return false;
@@ -93,7 +94,8 @@ void tune_store(const std::string &key, const BatchTune &t)
     std::lock_guard<std::mutex> lk(g_mu);
     load_locked();
     append_locked(gpu_name() + "|" + key, std::to_string(t.bs) + " " + std::to_string(t.ctas_per_sm) + " " +
-                                               std::to_string(t.rhs) + " " + std::to_string(t.spt));
+                                               std::to_string(t.rhs) + " " + std::to_string(t.spt) + " " +
+                                               std::to_string(t.p64));
 }
 
 bool tune_lookup_int(const std::string &key, int *out)

@@ -12,6 +12,7 @@ struct BatchTune {
     int ctas_per_sm;  // resident CTAs per SM of the persistent grid
     int rhs;          // right-hand sides per CTA: systems on one gauge field that share each link load (1,2,4,8)
     int spt;          // sites per thread: a tile is spt x bs sites
+    int p64;          // right-hand sides per pass of the FP64 dslash (1, 2, 4): link reuse against occupancy
 };
 
 bool tune_lookup(const std::string &key, BatchTune *out);

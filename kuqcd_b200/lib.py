@@ -65,7 +65,8 @@ EXPORTED_SYMBOLS = [
     "kq_spinor_bytes", "kq_spinor_upload", "kq_spinor_download", "kq_spinor_convert", "kq_dslash", "kq_mdagm",
     "kq_mdagm_noalloc", "kq_dslash_full", "kq_mdagm_full", "kq_long_links_compressed", "kq_slab_set",
     "kq_slab_face_bytes", "kq_slab_pack_faces", "kq_slab_link_face_bytes", "kq_slab_pack_link_face", "kq_slab_set_link_ghosts",
-    "kq_slab_dslash", "kq_field_axpby", "kq_field_dot", "kq_host_alloc", "kq_host_free", "kq_apply_host",
+    "kq_slab_dslash", "kq_slab_dslash_part", "kq_field_axpby", "kq_field_dot", "kq_field_dot_device",
+    "kq_field_ms_update", "kq_host_alloc", "kq_host_free", "kq_apply_host",
     "kq_vec_axpby", "kq_vec_dot",
     "kq_solve_multishift", "kq_solve_multishift_device", "kq_true_residuals", "kq_make_links_record",
     "kq_make_source_record", "kq_last_error", "kq_batch_create", "kq_batch_destroy", "kq_batch_add",
@@ -80,7 +81,8 @@ class BatchInfo(C.Structure):
     _fields_ = [("num_systems", C.c_int), ("iterations", C.c_int), ("batched_seconds", C.c_double),
                 ("kernel_launches", C.c_longlong), ("tile", C.c_int), ("ctas_per_sm", C.c_int),
                 ("max_true_residual", C.c_double), ("refined_systems", C.c_int), ("tuned_now", C.c_int),
-                ("rhs_per_cta", C.c_int), ("sites_per_thread", C.c_int), ("groups", C.c_int),
+                ("rhs_per_cta", C.c_int), ("sites_per_thread", C.c_int), ("fp64_rhs_per_pass", C.c_int),
+                ("groups", C.c_int),
                 ("check_seconds", C.c_double), ("refine_iterations", C.c_int)]
 
 _PKG = Path(__file__).resolve().parent
@@ -133,6 +135,9 @@ def library() -> C.CDLL:
         "kq_slab_dslash": (i, [vp, i, vp, vp, vp, vp, i, vp, d, vp]),
         "kq_field_axpby": (i, [vp, d, vp, d, vp, vp]),
         "kq_field_dot": (i, [vp, vp, vp, C.POINTER(d)]),
+        "kq_slab_dslash_part": (i, [vp, i, vp, vp, vp, vp, i, vp, d, i, vp]),
+        "kq_field_dot_device": (i, [vp, vp, vp, vp, vp]),
+        "kq_field_ms_update": (i, [vp, i, C.POINTER(d), C.POINTER(d), C.POINTER(d), vp, vp, vp, sz, vp]),
         "kq_solve_multishift": (i, [vp, C.POINTER(SolveParam), vp, C.POINTER(vp), C.POINTER(SolveInfo)]),
         "kq_solve_multishift_device": (i, [vp, C.POINTER(SolveParam), vp, vp, C.POINTER(SolveInfo)]),
         "kq_true_residuals": (i, [vp, i, i, C.POINTER(d), vp, vp, C.POINTER(d)]),

@@ -32,6 +32,10 @@ def _p(t):
     return L._ptr(t)
 
 
+# parts of a slab's output sites (kq_slab_dslash_part)
+PART_ALL, PART_INTERIOR, PART_BOUNDARY = 0, 1, 2
+
+
 # ---------------------------------------------------------------------------------------------------- host slicing
 def slab_of_links(record: np.ndarray, global_dims, rank: int, nranks: int) -> np.ndarray:
     """Local NORMAL_ORDER link record (even sites then odd sites, 72 values per site) of one rank's slab."""
@@ -62,9 +66,19 @@ class LocalTransport:
         R = len(faces)
         return [(faces[(r - 1) % R][1], faces[(r + 1) % R][0]) for r in range(R)]
 
+    def exchange_start(self, faces):
+        return faces
+
+    def exchange_wait(self, handle):
+        return self.exchange(handle)
+
     def allreduce(self, values):
         tot = np.sum(np.asarray(values, dtype=np.float64), axis=0)
         return [tot.copy() for _ in values]
+
+    def allreduce_device(self, tensors):
+        """Sum of the ranks' device tensors, returned on the host (one synchronisation)."""
+        return torch.stack([t for t in tensors]).sum(0).cpu().numpy()
 
 
 class TorchTransport:
@@ -83,16 +97,29 @@ class TorchTransport:
         return self.dist.get_global_rank(self.group, r) if self.group is not None else r
 
     def exchange(self, faces):
+        return self.exchange_wait(self.exchange_start(faces))
+
+    def exchange_start(self, faces):
+        """Posts the first phase (faces going up in t) and returns at once: work that reads no ghost (the interior
+        dslash) can run while it is in flight."""
         (lo, hi), = faces
         if self.world == 1:
-            return [(hi, lo)]
+            return (lo, hi, None, None, None)
         d = self.dist
         ghost_lo, ghost_hi = torch.empty_like(hi), torch.empty_like(lo)
         # up in t: my top face becomes the lower ghost of rank + 1
         ops = [d.P2POp(d.isend, hi, self._peer(1), self.group), d.P2POp(d.irecv, ghost_lo, self._peer(-1), self.group)]
-        for w in d.batch_isend_irecv(ops):
+        return (lo, hi, ghost_lo, ghost_hi, d.batch_isend_irecv(ops))
+
+    def exchange_wait(self, handle):
+        lo, hi, ghost_lo, ghost_hi, works = handle
+        if works is None:
+            return [(hi, lo)]
+        d = self.dist
+        for w in works:
             w.wait()
-        # down in t: my bottom face becomes the upper ghost of rank - 1
+        # down in t: my bottom face becomes the upper ghost of rank - 1 (a second phase, so that two ranks, whose
+        # neighbours are the same peer, match their messages in order)
         ops = [d.P2POp(d.isend, lo, self._peer(-1), self.group), d.P2POp(d.irecv, ghost_hi, self._peer(1), self.group)]
         for w in d.batch_isend_irecv(ops):
             w.wait()
@@ -107,6 +134,17 @@ class TorchTransport:
         t = torch.tensor(np.asarray(v, dtype=np.float64), device=dev)
         self.dist.all_reduce(t, group=self.group)
         return [t.cpu().numpy()]
+
+    def allreduce_device(self, tensors):
+        """One all-reduce of this rank's device tensor (NCCL on the device; gloo through the host), returned on the
+        host."""
+        (t,) = tensors
+        if self.dist.get_backend(self.group) != "nccl":
+            t = t.cpu()
+        else:
+            torch.cuda.synchronize()  # the local sums were written on the context's stream
+        self.dist.all_reduce(t, group=self.group)
+        return t.cpu().numpy()
 
 
 # ---------------------------------------------------------------------------------------------------- one slab
@@ -152,9 +190,23 @@ class Slab:
                       "kq_slab_pack_faces")
         return lo, hi
 
-    def dslash(self, prec, src, ghost_lo, ghost_hi, dst, dst_parity, pvec=None, sigma=0.0):
-        self.ctx._chk(L.library().kq_slab_dslash(self.ctx._h, prec, _p(src), _p(ghost_lo), _p(ghost_hi), _p(dst),
-                                                 dst_parity, _p(pvec), float(sigma), None), "kq_slab_dslash")
+    def dslash(self, prec, src, ghost_lo, ghost_hi, dst, dst_parity, pvec=None, sigma=0.0, part=PART_ALL):
+        self.ctx._chk(L.library().kq_slab_dslash_part(self.ctx._h, prec, _p(src), _p(ghost_lo), _p(ghost_hi),
+                                                      _p(dst), dst_parity, _p(pvec), float(sigma), part, None),
+                      "kq_slab_dslash_part")
+
+    def dot_device(self, x, y, out):
+        """local <x, y> into out (a one-element float64 device tensor), without a host round trip"""
+        self.ctx._chk(L.library().kq_field_dot_device(self.ctx._h, _p(x), _p(y), _p(out), None),
+                      "kq_field_dot_device")
+
+    def ms_update(self, B, Z, a, r, p_block, x_block, n):
+        """x_j -= B_j p_j ; p_j = Z_j r + a_j p_j for j < n (shift j's fields at block + j * field bytes)"""
+        vb = self.ctx.spinor_bytes(L.KUQCD_DOUBLE)
+        arr = [np.ascontiguousarray(v[:max(n, 1)], dtype=np.float64) for v in (B, Z, a)]
+        ptr = [v.ctypes.data_as(C.POINTER(C.c_double)) for v in arr]
+        self.ctx._chk(L.library().kq_field_ms_update(self.ctx._h, n, *ptr, _p(r), _p(p_block), _p(x_block), vb, None),
+                      "kq_field_ms_update")
 
     def axpby(self, a, x, b, y):
         self.ctx._chk(L.library().kq_field_axpby(self.ctx._h, float(a), _p(x), float(b), _p(y), None),
@@ -179,70 +231,86 @@ def exchange_link_ghosts(slabs, transport):
         s.set_link_ghosts(glo)
 
 
-def dslash(slabs, transport, prec, srcs, dsts, dst_parity, pvecs=None, sigma=0.0):
-    """dst_r = D src_r on every local slab (one halo exchange), or sigma * pvec_r - D src_r."""
+def dslash(slabs, transport, prec, srcs, dsts, dst_parity, pvecs=None, sigma=0.0, overlap=True):
+    """dst_r = D src_r on every local slab (one halo exchange), or sigma * pvec_r - D src_r.  With overlap, the
+    interior sites (which read no ghost) are computed while the faces are in flight, the boundary sites after they
+    have arrived -- the reference's StartComm / bulk loop / EndComm (dirac_hisq.cpp:412-414, 452-454)."""
     faces = [s.pack(prec, x) for s, x in zip(slabs, srcs)]
-    torch.cuda.synchronize()
-    ghosts = transport.exchange(faces)
+    torch.cuda.synchronize()  # faces packed before the transport reads them
+    handle = transport.exchange_start(faces)
+    pv = [None if pvecs is None else pvecs[k] for k in range(len(slabs))]
+    if overlap:
+        for k, (s, x, y) in enumerate(zip(slabs, srcs, dsts)):
+            s.dslash(prec, x, None, None, y, dst_parity, pv[k], sigma, part=PART_INTERIOR)
+    ghosts = transport.exchange_wait(handle)
     for k, (s, x, y, (glo, ghi)) in enumerate(zip(slabs, srcs, dsts, ghosts)):
-        s.dslash(prec, x, glo, ghi, y, dst_parity, None if pvecs is None else pvecs[k], sigma)
+        s.dslash(prec, x, glo, ghi, y, dst_parity, pv[k], sigma, part=PART_BOUNDARY if overlap else PART_ALL)
     torch.cuda.synchronize()
 
 
-def cgm(slabs, transport, bs, shifts_ref, tol, max_iter, parity=0):
+def cgm(slabs, transport, bs, shifts_ref, tol, max_iter, parity=0, overlap=True):
     """Multishift CG of inverter_cgm.cpp:17-87 on FP64 slab fields.  shifts_ref: reference semantics (x_0 solves
     shifts[0] - DD, x_j solves shifts[0] + shifts[j] - DD); stops shift k when Z_k^2 |r|^2 < tol.  Returns
-    (xs, iterations) with xs[r][k] the local solution of shift k on slab r."""
+    (xs, iterations) with xs[r][k] the local solution of shift k on slab r.
+
+    Per iteration: two dslash with overlapped halo exchange, two reductions -- each a device-side local sum and one
+    all-reduce over ranks (the reference's MPI_Allreduce, spinor_field.cpp:207-215, 235-243) -- the shifted scalar
+    recurrences vectorised over the shifts, and one fused pass over all shift vectors (kq_field_ms_update)."""
     ns = len(shifts_ref)
     D = L.KUQCD_DOUBLE
+    sh = np.asarray(shifts_ref, dtype=np.float64)
 
-    def allsum(vals):
-        return transport.allreduce([np.atleast_1d(np.asarray(v, dtype=np.float64)) for v in vals])[0]
+    def allsum(x, y):
+        outs = []
+        for s, xk, yk in zip(slabs, x, y):
+            o = torch.zeros(1, dtype=torch.float64, device=f"cuda:{s.device}")
+            s.dot_device(xk, yk, o)
+            outs.append(o)
+        return float(transport.allreduce_device(outs)[0])
 
+    vb = [s.ctx.spinor_bytes(D) for s in slabs]
     r = [s.field() for s in slabs]
     sv = [s.field() for s in slabs]
     tmp = [s.field() for s in slabs]
-    p = [[s.field() for _ in range(ns)] for s in slabs]
-    x = [[s.field() for _ in range(ns)] for s in slabs]
+    pblk = [torch.zeros(ns * n, dtype=torch.uint8, device=f"cuda:{s.device}") for s, n in zip(slabs, vb)]
+    xblk = [torch.zeros(ns * n, dtype=torch.uint8, device=f"cuda:{s.device}") for s, n in zip(slabs, vb)]
+    p0 = [pb[:n] for pb, n in zip(pblk, vb)]
     for k, s in enumerate(slabs):
         s.axpby(1.0, bs[k], 0.0, r[k])
         for j in range(ns):
-            s.axpby(1.0, bs[k], 0.0, p[k][j])
+            s.axpby(1.0, bs[k], 0.0, pblk[k][j * vb[k]:(j + 1) * vb[k]])
     a = np.zeros(ns)
     B = np.ones(ns)
     Z = np.ones(ns)
     Zm1 = np.ones(ns)
-    rr = float(allsum([s.dot(rk, rk) for s, rk in zip(slabs, r)])[0])
+    rr = allsum(r, r)
     Bm1, max_term, it = 1.0, ns, 0
     while True:
         it += 1
         # s = shifts[0] p0 - D_pq D_qp p0 (MdaggM + Axmy, inverter_cgm.cpp:44-46)
-        dslash(slabs, transport, D, [pk[0] for pk in p], tmp, 1 - parity)
-        dslash(slabs, transport, D, tmp, sv, parity, pvecs=[pk[0] for pk in p], sigma=shifts_ref[0])
-        pAp = float(allsum([s.dot(pk[0], sk) for s, pk, sk in zip(slabs, p, sv)])[0])
+        dslash(slabs, transport, D, p0, tmp, 1 - parity, overlap=overlap)
+        dslash(slabs, transport, D, tmp, sv, parity, pvecs=p0, sigma=shifts_ref[0], overlap=overlap)
+        pAp = allsum(p0, sv)
         B[0] = -rr / pAp
         for k, s in enumerate(slabs):
             s.axpby(B[0], sv[k], 1.0, r[k])
-        for j in range(1, max_term):
-            rr1 = Bm1 * Zm1[j] / (B[0] * a[0] * (Zm1[j] - Z[j]) + Zm1[j] * Bm1 * (1.0 - shifts_ref[j] * B[0]))
-            Zm1[j] = Z[j]
-            Z[j] = Z[j] * rr1
-            B[j] = B[0] * rr1
+        j = slice(1, max_term)
+        rr1 = Bm1 * Zm1[j] / (B[0] * a[0] * (Zm1[j] - Z[j]) + Zm1[j] * Bm1 * (1.0 - sh[j] * B[0]))
+        Zm1[j] = Z[j]
+        Z[j] = Z[j] * rr1
+        B[j] = B[0] * rr1
         Bm1 = B[0]
-        lam2 = float(allsum([s.dot(rk, rk) for s, rk in zip(slabs, r)])[0])
+        lam2 = allsum(r, r)
         a[0] = lam2 / rr
         rr = lam2
+        a[j] = a[0] * Z[j] * B[j] / (Zm1[j] * B[0])
+        # x_j -= B_j p_j ; p_j = Z_j r + a_j p_j  (Z_0 = 1), all shifts in one pass
         for k, s in enumerate(slabs):
-            for j in range(max_term):
-                s.axpby(-B[j], p[k][j], 1.0, x[k][j])
-        for j in range(1, max_term):
-            a[j] = a[0] * Z[j] * B[j] / (Zm1[j] * B[0])
-        for k, s in enumerate(slabs):
-            for j in range(max_term):
-                s.axpby(Z[j], r[k], a[j], p[k][j])
+            s.ms_update(B, Z, a, r[k], pblk[k], xblk[k], max_term)
         while max_term > 0 and Z[max_term - 1] ** 2 * lam2 < tol:
             max_term -= 1
         if max_term == 0 or it >= max_iter:
             break
     torch.cuda.synchronize()
+    x = [[xblk[k][j * vb[k]:(j + 1) * vb[k]] for j in range(ns)] for k in range(len(slabs))]
     return x, it

@@ -180,11 +180,12 @@ def test_batch_many_sources_on_one_field_match_single_system(cuda, tmp_path, mon
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("rhs,spt", [(1, 1), (2, 2), (4, 1), (8, 2)])
-def test_batch_groups_of_every_width(cuda, monkeypatch, rhs, spt):
-    """Every right-hand-sides-per-CTA width, set through KUQCD_BATCH_SHAPE, on groups that do not fill it: 3 sources
-    on one field (odd parity), 2 on another lattice, one system alone; all reach their targets."""
-    monkeypatch.setenv("KUQCD_BATCH_SHAPE", f"256,2,{rhs},{spt}")
+@pytest.mark.parametrize("rhs,spt,p64", [(1, 1, 1), (2, 2, 2), (4, 1, 4), (4, 2, 1), (8, 2, 2), (8, 1, 4)])
+def test_batch_groups_of_every_width(cuda, monkeypatch, rhs, spt, p64):
+    """Every right-hand-sides-per-CTA width and FP64 pass size, set through KUQCD_BATCH_SHAPE, on groups that do not
+    fill them: 3 sources on one field (odd parity), 2 on another lattice, one system alone; all reach their
+    targets."""
+    monkeypatch.setenv("KUQCD_BATCH_SHAPE", f"256,2,{rhs},{spt},{p64}")
     batch = K.Batch()
     keep = []
     for dims, eps, seed, n, parity in [((8, 8, 8, 8), 0.3, 31, 3, 1), ((8, 4, 4, 8), 0.35, 32, 2, 0),
@@ -197,6 +198,7 @@ def test_batch_groups_of_every_width(cuda, monkeypatch, rhs, spt):
             keep.append((ctx, fat, lng, vb, b, d_x, sig, parity, dims))
     info = batch.solve()
     assert info.tuned_now == 0 and info.rhs_per_cta == rhs and info.sites_per_thread == spt
+    assert info.fp64_rhs_per_pass == p64
     assert info.groups == sum((n + rhs - 1) // rhs for n in (3, 2, 1))
     for i, (ctx, fat, lng, vb, b, d_x, sig, parity, dims) in enumerate(keep):
         assert batch.system_info(i).status == 0, i
