@@ -429,6 +429,15 @@ def run_ours(args):
                 "dslash": small["dslash"], "gpu_launches": sm["launches"]}
             if small["plain_w"] is not None:
                 result["lattice_32"]["plain_fp64"]["windowed"] = plain_info(small["plain_w"], sm["ms"], world)
+        if small is not None and world == 1:
+            # the batched workloads (24 systems on three lattices), one timed step each after a warm-up step that
+            # includes the shape tuning: their own lines come from --config batch / batch-rhs
+            bargs = argparse.Namespace(**vars(args))
+            bargs.steps, bargs.warmup = 1, 1
+            for name, shared in (("batch", False), ("batch_rhs", True)):
+                b = run_batch(bargs, shared=shared, emit=False)
+                result[name] = {k: b[k] for k in ("value", "unit", "ms_per_step", "steps", "warmup", "config",
+                                                  "sequential", "gpu_launches", "clocks")}
         print(json.dumps(result))
     if world > 1:
         dist.barrier()
@@ -601,7 +610,7 @@ def run_reference(args):
     return res
 
 
-def run_batch(args, shared=False):
+def run_batch(args, shared=False, emit=True):
     """Batched multi-system workload: 24 systems, 8 each on 16^4, 24^3x48 and 32^4, own gauge field
     (eps ~ U[0.2,0.4]), own mass (m ~ U[0.01,0.1]), 8-16 shifts log-spaced 1e-4..1 and Gaussian source, all seeded.
     With shared=True (--config batch-rhs) the 8 systems of a lattice are 8 sources on one gauge field with one mass
@@ -702,7 +711,8 @@ def run_batch(args, shared=False):
                        "speedup_of_batched": t_s / t_b},
         "gpu_launches": int(info.kernel_launches), "clocks": clk.summary(),
     }
-    print(json.dumps(res))
+    if emit:
+        print(json.dumps(res))
     bobj.close()
     for ctx in set(c for c, *_ in systems):
         ctx.close()

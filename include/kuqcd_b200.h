@@ -238,7 +238,8 @@ typedef struct {
     int tuned_now;            /* 1 when this call measured the launch shape */
     int rhs_per_cta;          /* systems on one gauge field whose dslash shares each link load (1, 2, 4 or 8) */
     int sites_per_thread;     /* sites each thread handles per work item */
-    int fp64_rhs_per_pass;    /* right-hand sides the FP64 dslash serves per link load (1, 2 or 4) */
+    int fp64_rhs_per_pass;    /* right-hand sides the FP64 dslash serves per link load (1, 2 or 4); 0: all of a
+                                 group, spread over the warps with the links staged in shared memory */
     int groups;               /* groups of systems sharing link loads (+ systems solved on their own) */
     double check_seconds;     /* wall time of the batched systems' FP64 checks and refinements */
     int refine_iterations;    /* refinement iterations summed over the batched systems */

@@ -309,6 +309,297 @@ __global__ void __launch_bounds__(BS, Bounds<BS, M, Pass<M, R, P64>::v>::v) bk_d
     }
 }
 
+// ---------------------------------------------------------------------------- staged multi-RHS dslash (FP64)
+// The grouped kernels above hold every member's accumulators in one thread: with four FP64 members that is ~190
+// registers and one 256-thread CTA per SM, too few warps to cover the neighbour gathers.  The staged form spreads
+// the members over the warps instead: a CTA works on S = BS / R sites at a time (a round) and warp group r
+// (S / 32 warps) applies D to member r, so every thread keeps the single-system register footprint.  The four
+// links of one direction (fat and long, forward and backward) of the S sites are copied from global memory into
+// shared memory once -- warp group r copies every R-th 16-byte plane of them, with cp.async, so the copies hold no
+// registers -- and every member's threads decode their site's links from there.  Stages (round, direction) run in
+// a pipeline over two buffers: the next stage's copies are in flight while the current one is applied, one barrier
+// per stage.
+
+// A link in its storage form: n16 planes of 16 bytes, then a tail plane of tb bytes (FP64: 9 + 0, compressed
+// 6 + 8 (1/s); FP32: 4 + 8, compressed 3 + 4; HALF: 2 + 4); each plane pv sites long, one block per direction.
+template <int LP> __device__ __forceinline__ int form_n16(int recon)
+{
+    return LP == 0 ? (recon ? 6 : 9) : LP == 1 ? (recon ? 3 : 4) : 2;
+}
+template <int LP> __device__ __forceinline__ int form_tail(int recon)
+{
+    return LP == 0 ? (recon ? 8 : 0) : LP == 1 ? (recon ? 4 : 8) : 4;
+}
+template <int LP> __device__ __forceinline__ int form_bytes(int recon) { return 16 * form_n16<LP>(recon) + form_tail<LP>(recon); }
+template <int LP> struct LinkMaxBytes { static constexpr int v = LP == 0 ? 144 : LP == 1 ? 72 : 36; };
+// shared memory of one staged kernel: two stage buffers of four links per site
+template <int LP> constexpr size_t staged_smem(int S) { return (size_t)2 * 4 * LinkMaxBytes<LP>::v * S; }
+
+__device__ __forceinline__ void cp_async(void *sdst, const void *gsrc, int bytes)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+    if (bytes == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+    else if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gsrc) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// this thread's share of the link of site li (direction dir) into a stage buffer: planes r, r + R, ...; the tail if
+// n16 % R == r.  Sources and destinations are 16-byte aligned (pv is a multiple of 64, S of 32).
+template <int LP, int R>
+__device__ __forceinline__ void stage_link(char *sb, int S, int s, const void *par_base, int pv, int dir, int li,
+                                           int recon, int r)
+{
+    const int n16 = form_n16<LP>(recon), tb = form_tail<LP>(recon);
+    const char *d = static_cast<const char *>(par_base) + (size_t)dir * (16 * n16 + tb) * pv;
+    for (int k = r; k < n16; k += R) cp_async(sb + (k * S + s) * 16, d + ((size_t)k * pv + li) * 16, 16);
+    if (tb && n16 % R == r) cp_async(sb + n16 * 16 * S + s * tb, d + (size_t)n16 * 16 * pv + (size_t)li * tb, tb);
+}
+
+// the link of staged site s (same arithmetic as ld_link_fold: HALF values come back as raw int16)
+template <int LP, typename T>
+__device__ __forceinline__ void sm_link(const char *buf, int S, int s, int recon, T u[18])
+{
+    if constexpr (LP == 0) {
+        const int n = recon ? 6 : 9;
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+            if (k < n) {
+                const double2 w = reinterpret_cast<const double2 *>(buf + k * 16 * S)[s];
+                u[2 * k] = w.x;
+                u[2 * k + 1] = w.y;
+            }
+        if (recon) rebuild_row2(u, reinterpret_cast<const double *>(buf + 96 * S)[s]);
+    } else if constexpr (LP == 1) {
+        float w[18];
+        const int n = recon ? 3 : 4;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (k < n) {
+                const float4 a = reinterpret_cast<const float4 *>(buf + k * 16 * S)[s];
+                w[4 * k] = a.x; w[4 * k + 1] = a.y; w[4 * k + 2] = a.z; w[4 * k + 3] = a.w;
+            }
+        if (recon) {
+            rebuild_row2(w, reinterpret_cast<const float *>(buf + 48 * S)[s]);
+        } else {
+            const float2 a = reinterpret_cast<const float2 *>(buf + 64 * S)[s];
+            w[16] = a.x;
+            w[17] = a.y;
+        }
+#pragma unroll
+        for (int k = 0; k < 18; ++k) u[k] = (T)w[k];
+    } else {
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int4 a = reinterpret_cast<const int4 *>(buf + k * 16 * S)[s];
+            u[8 * k + 0] = lo16(a.x); u[8 * k + 1] = hi16(a.x);
+            u[8 * k + 2] = lo16(a.y); u[8 * k + 3] = hi16(a.y);
+            u[8 * k + 4] = lo16(a.z); u[8 * k + 5] = hi16(a.z);
+            u[8 * k + 6] = lo16(a.w); u[8 * k + 7] = hi16(a.w);
+        }
+        const int a = reinterpret_cast<const int *>(buf + 32 * S)[s];
+        u[16] = lo16(a);
+        u[17] = hi16(a);
+    }
+}
+
+// One staged pass over a (group, tile) item: for every round j (sites tile0 + j S + s) acc = (D src_r)(i) on output
+// parity p, then epi(i, acc) if this thread's member is applied and the site exists.  Every thread of the CTA calls
+// this.  Stage (j, d) holds direction d's links [fat at i | long at i | fat at i - mu | long at i - 3 mu] in
+// buffer d & 1.  The terms are those of dslash_site_t in the same order.
+template <int LP, int SP, typename T, int R, int S, typename Epi>
+__device__ __forceinline__ void staged_pass(const Geom &g, int pv, const LinkSet &fat, const LinkSet &lng,
+                                            const void *src, int p, int tile0, int rounds, int r, int s, bool mine,
+                                            char *buf0, char *buf1, Epi epi)
+{
+    const void *fat_p = p ? fat.par[1] : fat.par[0], *fat_q = p ? fat.par[0] : fat.par[1];
+    const void *lng_p = p ? lng.par[1] : lng.par[0], *lng_q = p ? lng.par[0] : lng.par[1];
+    const T rl = fold_scale_long<LP, T>(fat, lng);
+    const int fb = form_bytes<LP>(fat.recon) * S, lb = form_bytes<LP>(lng.recon) * S;
+    const int off[4] = {0, fb, fb + lb, 2 * fb + lb};  // link k of a stage buffer
+    auto site_of = [&](int j) {
+        const int i = tile0 + j * S + s;
+        return i < g.vh ? i : g.vh - 1;
+    };
+    auto issue = [&](char *sb, int dir, int i, const SiteCoord &c) {
+        stage_link<LP, R>(sb + off[0], S, s, fat_p, pv, dir, i, fat.recon, r);
+        stage_link<LP, R>(sb + off[1], S, s, lng_p, pv, dir, i, lng.recon, r);
+        stage_link<LP, R>(sb + off[2], S, s, fat_q, pv, dir, nbr_index(g, c, i, dir, -1), fat.recon, r);
+        stage_link<LP, R>(sb + off[3], S, s, lng_q, pv, dir, nbr_index(g, c, i, dir, -3), lng.recon, r);
+    };
+    int in = site_of(0);
+    SiteCoord cn = site_coord(g, in, p);
+    issue(buf0, 0, in, cn);
+    cp_async_commit();
+#pragma unroll 1
+    for (int j = 0; j < rounds; ++j) {
+        const int i = in;
+        const SiteCoord c = cn;
+        const bool work = mine && tile0 + j * S + s < g.vh;
+        T acc[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) acc[k] = T(0);
+#pragma unroll
+        for (int dir = 0; dir < 4; ++dir) {
+            char *cur = (dir & 1) ? buf1 : buf0, *nxt = (dir & 1) ? buf0 : buf1;
+            // stage (j, dir) has landed for every thread, and every thread is done with the buffer the next
+            // stage goes to (it held stage (j, dir - 1))
+            cp_async_wait_all();
+            __syncthreads();
+            if (dir < 3) {
+                issue(nxt, dir + 1, i, c);
+            } else if (j + 1 < rounds) {
+                in = site_of(j + 1);
+                cn = site_coord(g, in, p);
+                issue(nxt, 0, in, cn);
+            }
+            cp_async_commit();
+            if (work) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    T u[18], v[6];
+                    ld_spinor_as<SP>(src, pv, nbr_index(g, c, i, dir, k == 0 ? 1 : k == 1 ? 3 : k == 2 ? -1 : -3), v);
+                    sm_link<LP, T>(cur + off[k], S, s, (k & 1) ? lng.recon : fat.recon, u);
+                    if (k & 1) fold_long_spinor<LP>(rl, v);
+                    if (k < 2) mv_add(u, v, acc);
+                    else mdv_sub(u, v, acc);
+                }
+            }
+        }
+        if (work) {
+            fold_scale_site<LP>(fat, acc);
+            epi(i, acc);
+        }
+    }
+}
+
+// per-member partial sums of a tile: warp sums, then member r's S / 32 warps in order; thread 0 writes member r's
+// partial and the member's last tile runs the scalar step (`step`)
+template <int BS, int R, typename Step>
+__device__ __forceinline__ void staged_member_steps(const GroupDesc &G, unsigned use, int tile, double v,
+                                                    int ticket, double *wsum, double *sm, Step step)
+{
+    constexpr int WPM = BS / R / 32;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = v;
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        if (use & (1u << r)) {
+            const SysDesc &d = c_sys[G.mem[r]];
+            MsState *st = d.st;
+            if (threadIdx.x == 0) {
+                double a = 0.0;
+                for (int q = 0; q < WPM; ++q) a += wsum[r * WPM + q];
+                d.partials[tile] = a;
+            }
+            if (tile_ticket_last(&st->ticket[ticket], d.ntiles)) {
+                const double tot = tile_partials_sum(d.partials, d.ntiles, sm);
+                if (threadIdx.x < 32) {
+                    step(st, __shfl_sync(0xffffffffu, tot, 0));
+                    if (threadIdx.x == 0) st->ticket[ticket] = 0;
+                }
+            }
+            __syncthreads();
+        }
+}
+
+// rounds of a tile of spt BS sites on a lattice of vh sites per parity
+template <int BS, int S>
+__device__ __forceinline__ int staged_rounds(int tile0, int spt, int vh)
+{
+    const int left = vh - tile0;
+    const int n = (left + S - 1) / S;
+    return n < spt * (BS / S) ? n : spt * (BS / S);
+}
+
+// K1 (as bk_dslash1_kernel) with the members spread over the warps and the links staged in shared memory
+template <int BS, int M, int R>
+__global__ void __launch_bounds__(BS, Bounds<BS, M, 1>::v) bk_dslash1_staged_kernel(
+    const int2 *__restrict__ items, int nitems, int spt)
+{
+    typedef typename Acc2<M, M>::T T;
+    constexpr int S = BS / R;
+    static_assert(S % 32 == 0, "a member's sites fill whole warps");
+    extern __shared__ __align__(16) char dyn[];
+    char *buf0 = dyn, *buf1 = dyn + staged_smem<M>(S) / 2;
+    __shared__ double wsum[BS / 32], sm[32];
+    const int r = threadIdx.x / S, s = threadIdx.x % S;
+#pragma unroll 1
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int2 w = items[it];
+        const GroupDesc &G = c_grp[w.x];
+        const unsigned use = group_mask<R, M>(G);
+        if (!use) continue;
+        const SysDesc &d0 = c_sys[G.mem[0]];
+        const char *src = static_cast<const char *>(d0.p0) + r * d0.vb;
+        char *dst = static_cast<char *>(d0.tmp) + r * d0.vb;
+        const int tile0 = w.y * spt * BS;
+        double tt = 0.0;
+        staged_pass<M, 0, T, R, S>(d0.g, d0.pv, d0.fat[M], d0.lng[M], src, 1 - d0.parity, tile0,
+                                   staged_rounds<BS, S>(tile0, spt, d0.g.vh), r, s, (use >> r) & 1u, buf0, buf1,
+                                   [&](int i, const T acc[6]) {
+                                       st_spinor_as<M>(dst, d0.pv, i, acc);
+#pragma unroll
+                                       for (int k = 0; k < 6; ++k) tt += (double)acc[k] * (double)acc[k];
+                                   });
+        staged_member_steps<BS, R>(G, use, w.y, tt, 1, wsum, sm, [](MsState *st, double tot) {
+            ms_step_beta(st, st->shift[0] * st->pp + tot);
+        });
+    }
+}
+
+// K2 (as bk_dslash2_kernel), staged
+template <int BS, int M, int R>
+__global__ void __launch_bounds__(BS, Bounds<BS, M, 1>::v) bk_dslash2_staged_kernel(
+    const int2 *__restrict__ items, int nitems, int spt)
+{
+    typedef typename Acc2<M, M>::T T;
+    constexpr int S = BS / R;
+    static_assert(S % 32 == 0, "a member's sites fill whole warps");
+    extern __shared__ __align__(16) char dyn[];
+    char *buf0 = dyn, *buf1 = dyn + staged_smem<M>(S) / 2;
+    __shared__ double wsum[BS / 32], sm[32];
+    const int r = threadIdx.x / S, s = threadIdx.x % S;
+#pragma unroll 1
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int2 w = items[it];
+        const GroupDesc &G = c_grp[w.x];
+        const unsigned use = group_mask<R, M>(G);
+        if (!use) continue;
+        const SysDesc &d0 = c_sys[G.mem[0]];
+        const bool mine = (use >> r) & 1u;
+        const SysDesc &d = c_sys[G.mem[mine ? r : 0]];
+        const char *src = static_cast<const char *>(d0.tmp) + r * d0.vb;
+        const int tile0 = w.y * spt * BS;
+        double nn = 0.0;
+        staged_pass<M, M, T, R, S>(d0.g, d0.pv, d0.fat[M], d0.lng[M], src, d0.parity, tile0,
+                                   staged_rounds<BS, S>(tile0, spt, d0.g.vh), r, s, mine, buf0, buf1,
+                                   [&](int i, const T acc[6]) {
+                                       const MsState *st = d.st;
+                                       const int itc = st->iter;
+                                       const char *rin = static_cast<const char *>(d.ring) +
+                                                         (size_t)(itc % kWin) * d.vb;
+                                       char *rout = static_cast<char *>(d.ring) + (size_t)((itc + 1) % kWin) * d.vb;
+                                       double pv6[6], rv[6];
+                                       ld_spinor<0>(d.p0, d.pv, i, pv6);
+                                       ld_spinor<0>(rin, d.pv, i, rv);
+                                       const double sig = st->shift[0], b0 = st->B[0];
+#pragma unroll
+                                       for (int k = 0; k < 6; ++k) {
+                                           rv[k] += b0 * (sig * pv6[k] - (double)acc[k]);
+                                           nn += rv[k] * rv[k];
+                                       }
+                                       st_spinor<0>(rout, d.pv, i, rv);
+                                   });
+        staged_member_steps<BS, R>(G, use, w.y, nn, 2, wsum, sm,
+                                   [](MsState *st, double tot) { ms_step_alpha(st, tot); });
+    }
+}
+
 // K3: p0 = r^(i) + a0 p0; the next iteration's precision takes effect.  A system that stopped in K2 no longer
 // needs p0.
 template <int BS>
@@ -394,15 +685,46 @@ static void enqueue_batch_init(const BatchItems &it, int grid, int spt, cudaStre
     bk_init_kernel<BS><<<grid, BS, 0, s>>>(it.sys, it.nsys, spt);
 }
 
+// the staged FP64 kernels need whole warps per member: R in 2..BS / 32
+constexpr bool staged_ok(int bs, int r) { return r > 1 && (bs / r) % 32 == 0; }
+
+// the staged kernels' dynamic shared memory (two stage buffers: up to 144 KB for 128 sites per round)
+template <int BS, int R>
+static cudaError_t staged_attr()
+{
+    if constexpr (staged_ok(BS, R)) {
+        const int sm = (int)staged_smem<0>(BS / R);
+        KQ_CUDA_TRY(cudaFuncSetAttribute(bk_dslash1_staged_kernel<BS, 0, R>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        KQ_CUDA_TRY(cudaFuncSetAttribute(bk_dslash2_staged_kernel<BS, 0, R>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    }
+    return cudaSuccess;
+}
+
+static cudaError_t staged_attrs()
+{
+    KQ_CUDA_TRY((staged_attr<128, 2>()));
+    KQ_CUDA_TRY((staged_attr<128, 4>()));
+    KQ_CUDA_TRY((staged_attr<256, 2>()));
+    KQ_CUDA_TRY((staged_attr<256, 4>()));
+    KQ_CUDA_TRY((staged_attr<256, 8>()));
+    return cudaSuccess;
+}
+
 template <int BS, int R, int P64>
 static void enqueue_batch_chunk_r(const BatchItems &it, int grid, int spt, cudaStream_t s)
 {
     for (int k = 0; k < kChunk; ++k) {
-        // (P64 only shapes the FP64 kernels; the sloppy ones are instantiated once)
-        bk_dslash1_kernel<BS, 0, R, P64><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
+        // (P64 only shapes the FP64 kernels, 0 = staged; the sloppy ones are instantiated once)
+        if constexpr (P64 == 0)
+            bk_dslash1_staged_kernel<BS, 0, R><<<grid, BS, staged_smem<0>(BS / R), s>>>(it.grp, it.ngrp, spt);
+        else bk_dslash1_kernel<BS, 0, R, P64><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
         bk_dslash1_kernel<BS, 1, R, 1><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
         bk_dslash1_kernel<BS, 2, R, 1><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
-        bk_dslash2_kernel<BS, 0, R, P64><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
+        if constexpr (P64 == 0)
+            bk_dslash2_staged_kernel<BS, 0, R><<<grid, BS, staged_smem<0>(BS / R), s>>>(it.grp, it.ngrp, spt);
+        else bk_dslash2_kernel<BS, 0, R, P64><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
         bk_dslash2_kernel<BS, 1, R, 1><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
         bk_dslash2_kernel<BS, 2, R, 1><<<grid, BS, 0, s>>>(it.grp, it.ngrp, spt);
         bk_p0_kernel<BS><<<grid, BS, 0, s>>>(it.sys, it.nsys, spt);
@@ -413,6 +735,11 @@ static void enqueue_batch_chunk_r(const BatchItems &it, int grid, int spt, cudaS
 template <int BS, int R>
 static void enqueue_batch_chunk_p(const BatchItems &it, int grid, int spt, int p64, cudaStream_t s)
 {
+    if constexpr (staged_ok(BS, R))
+        if (p64 == 0) {
+            enqueue_batch_chunk_r<BS, R, 0>(it, grid, spt, s);
+            return;
+        }
     if (R == 1 || p64 == 1) enqueue_batch_chunk_r<BS, R, 1>(it, grid, spt, s);
     else if (R == 2 || p64 == 2) enqueue_batch_chunk_r<BS, R, 2>(it, grid, spt, s);
     else enqueue_batch_chunk_r<BS, R, 4>(it, grid, spt, s);
@@ -667,9 +994,13 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
     int dev_sms = 148;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, b->device);
     const int shared = max_shared(b->sys);
+    if (const cudaError_t e = staged_attrs(); e != cudaSuccess) {
+        set_last_error(std::string("kq_batch_solve: ") + cudaGetErrorString(e));
+        return status_of(e);
+    }
 
     // launch shape: tuned once per batch signature (sizes, shared gauge fields, shifts, schedule), cached on disk
-    std::string key = "batch3";
+    std::string key = "batch4";
     for (auto &S : b->sys) {
         int owner = 0;  // first system on the same context: systems sharing links share this number
         while (b->sys[owner].ctx != S.ctx) ++owner;
@@ -687,7 +1018,7 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
         if (n == 4) t.p64 = t.rhs < 4 ? t.rhs : 4;
         if (n >= 4 && (t.bs == 128 || t.bs == 256) && t.ctas_per_sm >= 1 && t.ctas_per_sm <= 32 &&
             (t.rhs == 1 || t.rhs == 2 || t.rhs == 4 || t.rhs == 8) && (t.spt == 1 || t.spt == 2) &&
-            (t.p64 == 1 || t.p64 == 2 || t.p64 == 4)) {
+            (t.p64 == 1 || t.p64 == 2 || t.p64 == 4 || (t.p64 == 0 && staged_ok(t.bs, t.rhs)))) {
             tune = t;
             have_tune = true;
         }
@@ -820,6 +1151,18 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
         for (int p = 1; p < std::min(t.rhs, 4); p *= 2) {
             BatchTune c = t;
             c.p64 = p;
+            const cudaError_t e = trial(c);
+            if (e != cudaSuccess) return status_of(e);
+        }
+        // the staged FP64 kernels (every member at the single-system occupancy, links shared through shared
+        // memory), at the chosen group width and at the widest one
+        t = tune;
+        const int widths[2] = {t.rhs, rmax};
+        for (int q = 0; q < 2; ++q) {
+            if ((q == 1 && widths[1] == widths[0]) || !staged_ok(t.bs, widths[q])) continue;
+            BatchTune c = t;
+            c.rhs = widths[q];
+            c.p64 = 0;
             const cudaError_t e = trial(c);
             if (e != cudaSuccess) return status_of(e);
         }

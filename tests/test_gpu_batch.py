@@ -180,11 +180,13 @@ def test_batch_many_sources_on_one_field_match_single_system(cuda, tmp_path, mon
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("rhs,spt,p64", [(1, 1, 1), (2, 2, 2), (4, 1, 4), (4, 2, 1), (8, 2, 2), (8, 1, 4)])
+@pytest.mark.parametrize("rhs,spt,p64", [(1, 1, 1), (2, 2, 2), (4, 1, 4), (4, 2, 1), (8, 2, 2), (8, 1, 4),
+                                         (2, 1, 0), (4, 2, 0), (8, 1, 0)])
 def test_batch_groups_of_every_width(cuda, monkeypatch, rhs, spt, p64):
-    """Every right-hand-sides-per-CTA width and FP64 pass size, set through KUQCD_BATCH_SHAPE, on groups that do not
-    fill them: 3 sources on one field (odd parity), 2 on another lattice, one system alone; all reach their
-    targets."""
+    """Every right-hand-sides-per-CTA width and FP64 pass size (0: the staged FP64 kernels, members spread over the
+    warps and links shared through shared memory), set through KUQCD_BATCH_SHAPE, on groups that do not fill them:
+    3 sources on one field (odd parity), 2 on another lattice, one system alone, lattices whose half volume is not
+    a multiple of the staged round; all reach their targets."""
     monkeypatch.setenv("KUQCD_BATCH_SHAPE", f"256,2,{rhs},{spt},{p64}")
     batch = K.Batch()
     keep = []
