@@ -1000,7 +1000,7 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
     }
 
     // launch shape: tuned once per batch signature (sizes, shared gauge fields, shifts, schedule), cached on disk
-    std::string key = "batch4";
+    std::string key = "batch5";
     for (auto &S : b->sys) {
         int owner = 0;  // first system on the same context: systems sharing links share this number
         while (b->sys[owner].ctx != S.ctx) ++owner;
@@ -1109,21 +1109,21 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
     };
 
     if (!have_tune) {
-        // Time two windows of the real batch per candidate shape (the solve restarts afterwards), one dimension
-        // at a time: tile x CTAs per SM with every shared gauge field serving as many right-hand sides as it can,
-        // then the right-hand sides per CTA, then the sites per thread.
-        float best = 1e30f;
-        auto trial = [&](BatchTune t) -> cudaError_t {
-            float ms = 0;
+        // Time the real batch per candidate shape (the solve restarts afterwards), one dimension at a time: tile x
+        // CTAs per SM on two windows, with every shared gauge field serving as many right-hand sides as it can;
+        // per group width, the FP64 pass mode on two windows (the solve's first windows run on FP64 links); the
+        // group widths against each other on complete solves (the width also sets the sloppy kernels' register
+        // use, which the first windows do not see); then the sites per thread.
+        auto timed = [&](const BatchTune &t, int chunks, float *ms) -> cudaError_t {
             long long l = 0;
             int ch = 0, ng = 0;
-            const cudaError_t e = run(t, 2, &ms, &l, &ch, &ng);
-            if (e == cudaSuccess && ch > 0 && ms < best) {
-                best = ms;
-                tune = t;
-            }
+            *ms = 1e30f;
+            float m = 0;
+            const cudaError_t e = run(t, chunks, &m, &l, &ch, &ng);
+            if (e == cudaSuccess && ch > 0) *ms = m;
             return e;
         };
+        float best = 1e30f;
         int rmax = 1;
         while (rmax < std::min(shared, kMaxR)) rmax *= 2;
         BatchTune t{256, 4, rmax, 1, std::min(rmax, 4)};
@@ -1131,45 +1131,57 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
         for (int bs : bss)
             for (int cps : cpss) {
                 if (bs == 256 && cps > 8) continue;
-                t.bs = bs;
-                t.ctas_per_sm = cps;
-                const cudaError_t e = trial(t);
+                BatchTune c = t;
+                c.bs = bs;
+                c.ctas_per_sm = cps;
+                float ms;
+                const cudaError_t e = timed(c, 2, &ms);
                 if (e != cudaSuccess) return status_of(e);
+                if (ms < best) {
+                    best = ms;
+                    tune = c;
+                }
             }
-        t = tune;
-        for (int r = 1; r <= rmax; r *= 2) {
-            if (r == t.rhs) continue;
-            BatchTune c = t;
-            c.rhs = r;
-            c.p64 = std::min(r, 4);
-            const cudaError_t e = trial(c);
-            if (e != cudaSuccess) return status_of(e);
+        if (rmax > 1) {
+            const BatchTune base = tune;
+            best = 1e30f;
+            for (int r = 1; r <= rmax; r *= 2) {
+                // FP64 pass modes of this width: members per pass 1, 2, 4 (up to r) and the staged kernels
+                int modes[4], nm = 0;
+                for (int p = 1; p <= std::min(r, 4); p *= 2) modes[nm++] = p;
+                if (staged_ok(base.bs, r)) modes[nm++] = 0;
+                BatchTune wbest = base;
+                float wms = 1e30f;
+                for (int q = 0; q < nm; ++q) {
+                    BatchTune c = base;
+                    c.rhs = r;
+                    c.p64 = modes[q];
+                    float ms;
+                    const cudaError_t e = nm > 1 ? timed(c, 2, &ms) : cudaSuccess;
+                    if (e != cudaSuccess) return status_of(e);
+                    if (nm == 1 || ms < wms) {
+                        wms = ms;
+                        wbest = c;
+                    }
+                }
+                float ms;
+                const cudaError_t e = timed(wbest, 0, &ms);
+                if (e != cudaSuccess) return status_of(e);
+                if (ms < best) {
+                    best = ms;
+                    tune = wbest;
+                }
+            }
         }
-        // FP64 right-hand sides per pass, below the full group: occupancy against link reuse in the FP64 phase (the
-        // timed windows are the solve's first, which run on FP64 links)
-        t = tune;
-        for (int p = 1; p < std::min(t.rhs, 4); p *= 2) {
-            BatchTune c = t;
-            c.p64 = p;
-            const cudaError_t e = trial(c);
+        {
+            BatchTune c = tune;
+            c.spt = 2;
+            float ms1, ms2;
+            cudaError_t e = timed(tune, 2, &ms1);
+            if (e == cudaSuccess) e = timed(c, 2, &ms2);
             if (e != cudaSuccess) return status_of(e);
+            if (ms2 < ms1) tune = c;
         }
-        // the staged FP64 kernels (every member at the single-system occupancy, links shared through shared
-        // memory), at the chosen group width and at the widest one
-        t = tune;
-        const int widths[2] = {t.rhs, rmax};
-        for (int q = 0; q < 2; ++q) {
-            if ((q == 1 && widths[1] == widths[0]) || !staged_ok(t.bs, widths[q])) continue;
-            BatchTune c = t;
-            c.rhs = widths[q];
-            c.p64 = 0;
-            const cudaError_t e = trial(c);
-            if (e != cudaSuccess) return status_of(e);
-        }
-        BatchTune c = tune;
-        c.spt = 2;
-        const cudaError_t e = trial(c);
-        if (e != cudaSuccess) return status_of(e);
         tune_store(key, tune);
     }
     float ms = 0;

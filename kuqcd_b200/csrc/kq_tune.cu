@@ -80,7 +80,7 @@ bool tune_lookup(const std::string &key, BatchTune *out)
     std::istringstream is(it->second);
     BatchTune t;
     if (!(is >> t.bs >> t.ctas_per_sm >> t.rhs >> t.spt >> t.p64)) return false;
-    if (t.p64 != 1 && t.p64 != 2 && t.p64 != 4) return false;
+    if (t.p64 != 0 && t.p64 != 1 && t.p64 != 2 && t.p64 != 4) return false;  // 0: staged FP64 kernels
     if (t.bs != 128 && t.bs != 256) return false;
     if (t.ctas_per_sm < 1 || t.ctas_per_sm > 32) return false;
     if (t.rhs != 1 && t.rhs != 2 && t.rhs != 4 && t.rhs != 8) return false;

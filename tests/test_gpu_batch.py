@@ -176,6 +176,11 @@ def test_batch_many_sources_on_one_field_match_single_system(cuda, tmp_path, mon
             r = O.true_residual(dims, fat, lng, 0, s, b, xb)
             assert r <= (1.2e-10 if solver == K.KQ_SOLVER_MIXED else 1.5e-10), (j, k, r)
             assert np.abs(xb - ref[k]).max() <= 1e-9 * np.abs(ref[k]).max(), (j, k)
+    # the tuned shape, whichever FP64 pass mode it has, comes back from the cache
+    info2 = batch.solve()
+    assert info2.tuned_now == 0
+    assert (info2.rhs_per_cta, info2.sites_per_thread, info2.fp64_rhs_per_pass) == \
+        (info.rhs_per_cta, info.sites_per_thread, info.fp64_rhs_per_pass)
     batch.close()
 
 
