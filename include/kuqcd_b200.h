@@ -158,6 +158,35 @@ KuQCDStatus kq_field_dot_device(kq_context *ctx, const void *d_x, const void *d_
  * x_j -= B_j p_j, then p_j = Z_j r + a_j p_j; shift j's FP64 fields at d_p + j * stride and d_x + j * stride */
 KuQCDStatus kq_field_ms_update(kq_context *ctx, int num_shift, const double *B, const double *Z, const double *a,
                                const void *d_r, void *d_p, void *d_x, size_t stride, void *stream);
+/* Device-driven multishift CG over slabs: the recurrences of CGM::Invert (inverter_cgm.cpp:17-87) on a state in
+ * device memory, so that no step waits on the host.  Per iteration, in stream order on every rank:
+ *   s = shifts_ref[0] p_0 - D D p_0 (two kq_slab_dslash with the halo exchange);
+ *   kq_field_dot_device(p_0, s, &state->sums[0]); the caller all-reduces sums[0] in place over ranks;
+ *   kq_slab_cgm_step(KQ_CGM_ALPHA); kq_slab_cgm_residual(s, r)   (r += B_0 s, local |r|^2 -> sums[1]);
+ *   the caller all-reduces sums[1]; kq_slab_cgm_step(KQ_CGM_BETA); kq_slab_cgm_update(r, p, x);
+ *   kq_slab_cgm_step(KQ_CGM_FINISH)   (drops converged shifts, counts the iteration, sets done).
+ * Before the first iteration: r = p_j = b, kq_field_dot_device(r, r, &sums[1]), all-reduce, KQ_CGM_START.  Once
+ * done is set every step is a no-op, so several iterations may be enqueued between two kq_slab_cgm_poll calls; the
+ * iteration count is the reference's.  shifts_ref have the reference's meaning (shift 0 absolute, shift j relative
+ * to it); shift j stops when Z_j^2 |r|^2 < tol.  d_state: kq_slab_cgm_state_bytes() of device memory, 8-byte
+ * aligned. */
+typedef struct {
+    double sums[2]; /* [0] <p_0, A p_0>, [1] |r|^2: local sums from the library, all-reduced in place by the caller */
+    double rr, Bm1, tol;
+    int iter, max_iter, num_shift, max_term, done, reserved;
+    double sh[64], a[64], B[64], Z[64], Zm1[64];
+} kq_slab_cgm_state;
+enum { KQ_CGM_START = 0, KQ_CGM_ALPHA = 1, KQ_CGM_BETA = 2, KQ_CGM_FINISH = 3 };
+size_t kq_slab_cgm_state_bytes(void);
+KuQCDStatus kq_slab_cgm_init(kq_context *ctx, kq_slab_cgm_state *d_state, int num_shift, const double *shifts_ref,
+                             double tol, int max_iter, void *stream);
+KuQCDStatus kq_slab_cgm_step(kq_context *ctx, kq_slab_cgm_state *d_state, int step, void *stream);
+KuQCDStatus kq_slab_cgm_residual(kq_context *ctx, kq_slab_cgm_state *d_state, const void *d_s, void *d_r,
+                                 void *stream);
+KuQCDStatus kq_slab_cgm_update(kq_context *ctx, const kq_slab_cgm_state *d_state, const void *d_r, void *d_p,
+                               void *d_x, size_t stride, void *stream);
+/* iterations so far and whether the solve has stopped (waits for the stream) */
+KuQCDStatus kq_slab_cgm_poll(kq_context *ctx, const kq_slab_cgm_state *d_state, int *iter, int *done, void *stream);
 
 /* ---------------------------------------------------------------- solver */
 enum {

@@ -16,6 +16,8 @@
 // of t links (kq_slab_pack_link_face), the caller delivers them once after loading, and kq_slab_set_link_ghosts
 // stores them (FP64, with an FP32 copy made on first use).
 #include <algorithm>
+#include <cstddef>
+#include <cstdint>
 #include <vector>
 
 #include "kq_context.h"
@@ -522,4 +524,222 @@ KQ_API KuQCDStatus kq_field_dot(kq_context *ctx, const void *d_x, const void *d_
     for (double v : h) sum += v;
     *out = sum;
     return status_of(e);
+}
+
+// ------------------------------------------------------------------------------------ device-driven multishift CG
+// The CGM recurrences of inverter_cgm.cpp:17-87 on a device state, so that a solve over slabs never waits on the
+// host: the local sums go to state->sums (sums[0] = <p, A p>, sums[1] = |r|^2), the caller all-reduces them in place
+// on the device in stream order, and every step reads its scalars from the state.  Once the solve has stopped
+// (state->done) every step is a no-op, so a caller may enqueue several iterations between two polls.
+static_assert(offsetof(kq_slab_cgm_state, iter) == 40 && sizeof(kq_slab_cgm_state) == 2624,
+              "kq_slab_cgm_state layout (read by hosts through kq_slab_cgm_poll)");
+
+struct CgmInit {
+    int ns, max_iter;
+    double tol;
+    double sh[kMaxShift];
+};
+
+__global__ void slab_cgm_init_kernel(kq_slab_cgm_state *st, CgmInit in)
+{
+    const int j = threadIdx.x;
+    if (j == 0) {
+        st->sums[0] = st->sums[1] = 0.0;
+        st->rr = 0.0;
+        st->Bm1 = 1.0;
+        st->tol = in.tol;
+        st->iter = 0;
+        st->max_iter = in.max_iter;
+        st->num_shift = in.ns;
+        st->max_term = in.ns;
+        st->done = 0;
+        st->reserved = 0;
+    }
+    for (int k = j; k < kMaxShift; k += blockDim.x) {
+        st->sh[k] = k < in.ns ? in.sh[k] : 0.0;
+        st->a[k] = 0.0;
+        st->B[k] = st->Z[k] = st->Zm1[k] = 1.0;
+    }
+}
+
+// one block of kMaxShift threads; thread j updates shift j (the vectorised loop over shifts of inverter_cgm.cpp:49-60)
+__global__ void slab_cgm_step_kernel(kq_slab_cgm_state *st, int step)
+{
+    if (st->done) return;  // uniform over the block
+    const int j = threadIdx.x;
+    if (step == KQ_CGM_START) {
+        // |b|^2 = 0: x = 0 solves every shift; a non-finite source stops at once
+        if (j == 0) {
+            st->rr = st->sums[1];
+            if (!(st->rr > 0.0) || !isfinite(st->rr)) st->done = 1;
+        }
+    } else if (step == KQ_CGM_ALPHA) {
+        // B_0 = -|r|^2 / <p, A p>; the shifted B_j, Z_j with the previous a_0 and B_0 (inverter_cgm.cpp:47-57)
+        const double B0 = -st->rr / st->sums[0], a0 = st->a[0], Bm1 = st->Bm1;
+        if (j >= 1 && j < st->max_term) {
+            const double z = st->Z[j], zm1 = st->Zm1[j];
+            const double rr1 = Bm1 * zm1 / (B0 * a0 * (zm1 - z) + zm1 * Bm1 * (1.0 - st->sh[j] * B0));
+            st->Zm1[j] = z;
+            st->Z[j] = z * rr1;
+            st->B[j] = B0 * rr1;
+        }
+        __syncthreads();
+        if (j == 0) {
+            st->B[0] = B0;
+            st->Bm1 = B0;
+        }
+    } else if (step == KQ_CGM_BETA) {
+        // a_0 = |r_new|^2 / |r|^2 and the shifted a_j (inverter_cgm.cpp:58-66)
+        const double lam2 = st->sums[1], a0 = lam2 / st->rr, B0 = st->B[0];
+        if (j >= 1 && j < st->max_term) st->a[j] = a0 * st->Z[j] * st->B[j] / (st->Zm1[j] * B0);
+        __syncthreads();
+        if (j == 0) {
+            st->a[0] = a0;
+            st->rr = lam2;
+        }
+    } else if (j == 0) {  // KQ_CGM_FINISH: drop converged shifts from the end (inverter_cgm.cpp:70-80)
+        int mt = st->max_term;
+        while (mt > 0 && st->Z[mt - 1] * st->Z[mt - 1] * st->rr < st->tol) --mt;
+        st->max_term = mt;
+        st->iter += 1;
+        st->done = (mt == 0 || st->iter >= st->max_iter) ? 1 : 0;
+    }
+}
+
+// r += B_0 s and the block partials of |r|^2
+__global__ void slab_cgm_residual_kernel(int vh, int pv, const kq_slab_cgm_state *st, const void *__restrict__ s_,
+                                         void *r_, double *partials)
+{
+    __shared__ double sm[32];
+    if (st->done) return;  // uniform over the grid
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double nn = 0.0;
+    if (i < vh) {
+        const double b0 = st->B[0];
+        double sv[6], rv[6];
+        ld_spinor<0>(s_, pv, i, sv);
+        ld_spinor<0>(r_, pv, i, rv);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            rv[k] += b0 * sv[k];
+            nn += rv[k] * rv[k];
+        }
+        st_spinor<0>(r_, pv, i, rv);
+    }
+    nn = block_sum(nn, sm);
+    if (threadIdx.x == 0) partials[blockIdx.x] = nn;
+}
+
+__global__ void slab_cgm_sum_kernel(const kq_slab_cgm_state *st, const double *__restrict__ partials, int n,
+                                    double *out)
+{
+    __shared__ double sm[32];
+    if (st->done) return;
+    double s = 0.0;
+    for (int b = threadIdx.x; b < n; b += blockDim.x) s += partials[b];
+    s = block_sum(s, sm);
+    if (threadIdx.x == 0) *out = s;
+}
+
+// x_j -= B_j p_j ; p_j = Z_j r + a_j p_j for the shifts still iterating, coefficients from the state
+__global__ void slab_cgm_update_kernel(int vh, int pv, const kq_slab_cgm_state *st, const void *__restrict__ r,
+                                       char *p, char *x, size_t stride)
+{
+    if (st->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= vh) return;
+    const int n = st->max_term;
+    double rv[6];
+    ld_spinor<0>(r, pv, i, rv);
+    for (int j = 0; j < n; ++j) {
+        const double B = st->B[j], Z = st->Z[j], a = st->a[j];
+        double pv6[6], xv[6];
+        ld_spinor<0>(p + j * stride, pv, i, pv6);
+        ld_spinor<0>(x + j * stride, pv, i, xv);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            xv[k] -= B * pv6[k];
+            pv6[k] = Z * rv[k] + a * pv6[k];
+        }
+        st_spinor<0>(x + j * stride, pv, i, xv);
+        st_spinor<0>(p + j * stride, pv, i, pv6);
+    }
+}
+
+KQ_API size_t kq_slab_cgm_state_bytes(void) { return sizeof(kq_slab_cgm_state); }
+
+KQ_API KuQCDStatus kq_slab_cgm_init(kq_context *ctx, kq_slab_cgm_state *d_state, int num_shift,
+                                    const double *shifts_ref, double tol, int max_iter, void *stream)
+{
+    if (!ctx || !d_state || !shifts_ref) return KUQCD_ERR_NULL_POINTER;
+    if (num_shift < 1 || num_shift > kMaxShift || max_iter < 1) return KUQCD_ERR_INVALID_PARAM;
+    if ((reinterpret_cast<uintptr_t>(d_state) & 7) != 0) return KUQCD_ERR_INVALID_PARAM;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    CgmInit in;
+    in.ns = num_shift;
+    in.max_iter = max_iter;
+    in.tol = tol;
+    for (int j = 0; j < kMaxShift; ++j) in.sh[j] = j < num_shift ? shifts_ref[j] : 0.0;
+    slab_cgm_init_kernel<<<1, kMaxShift, 0, s>>>(d_state, in);
+    return status_of(cudaGetLastError());
+}
+
+KQ_API KuQCDStatus kq_slab_cgm_step(kq_context *ctx, kq_slab_cgm_state *d_state, int step, void *stream)
+{
+    if (!ctx || !d_state) return KUQCD_ERR_NULL_POINTER;
+    if (step < KQ_CGM_START || step > KQ_CGM_FINISH) return KUQCD_ERR_INVALID_PARAM;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    slab_cgm_step_kernel<<<1, kMaxShift, 0, s>>>(d_state, step);
+    return status_of(cudaGetLastError());
+}
+
+KQ_API KuQCDStatus kq_slab_cgm_residual(kq_context *ctx, kq_slab_cgm_state *d_state, const void *d_s, void *d_r,
+                                        void *stream)
+{
+    if (!ctx || !d_state || !d_s || !d_r) return KUQCD_ERR_NULL_POINTER;
+    cudaSetDevice(ctx->device);
+    const Geom &g = ctx->g;
+    const int nb = (g.vh + 255) / 256;
+    Carve probe(nullptr);
+    probe.take(sizeof(double) * nb);
+    cudaError_t e = ensure_work(ctx, probe.off);
+    if (e != cudaSuccess) return status_of(e);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    double *partials = static_cast<double *>(ctx->work);
+    slab_cgm_residual_kernel<<<nb, 256, 0, s>>>(g.vh, pad_sites(g.vh), d_state, d_s, d_r, partials);
+    slab_cgm_sum_kernel<<<1, 256, 0, s>>>(d_state, partials, nb, &d_state->sums[1]);
+    return status_of(cudaGetLastError());
+}
+
+KQ_API KuQCDStatus kq_slab_cgm_update(kq_context *ctx, const kq_slab_cgm_state *d_state, const void *d_r, void *d_p,
+                                      void *d_x, size_t stride, void *stream)
+{
+    if (!ctx || !d_state || !d_r || !d_p || !d_x) return KUQCD_ERR_NULL_POINTER;
+    cudaSetDevice(ctx->device);
+    const Geom &g = ctx->g;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    slab_cgm_update_kernel<<<(g.vh + 255) / 256, 256, 0, s>>>(g.vh, pad_sites(g.vh), d_state, d_r,
+                                                              static_cast<char *>(d_p), static_cast<char *>(d_x),
+                                                              stride);
+    return status_of(cudaGetLastError());
+}
+
+KQ_API KuQCDStatus kq_slab_cgm_poll(kq_context *ctx, const kq_slab_cgm_state *d_state, int *iter, int *done,
+                                    void *stream)
+{
+    if (!ctx || !d_state || !iter || !done) return KUQCD_ERR_NULL_POINTER;
+    cudaSetDevice(ctx->device);
+    int h[5] = {0, 0, 0, 0, 0};  // iter, max_iter, num_shift, max_term, done
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    cudaError_t e = cudaMemcpyAsync(h, &d_state->iter, sizeof(h), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        set_last_error(std::string("kq_slab_cgm_poll: ") + cudaGetErrorString(e));
+        return status_of(e);
+    }
+    *iter = h[0];
+    *done = h[4];
+    return KUQCD_SUCCESS;
 }

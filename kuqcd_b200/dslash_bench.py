@@ -5,6 +5,12 @@ M = N^dag N (N: 1 -> 8 -> 8 channels, random weights) instead, four tensor-core 
 
     python -m kuqcd_b200.dslash_bench --dims 32 32 32 32 --prec double --reps 20
     python -m kuqcd_b200.dslash_bench --dims 32 32 32 32 --ptc --reps 5
+
+With --batch-sources N it solves N seeded sources on the one gauge field together with kq_batch_solve (mixed
+solver, 12 shifts, per-shift true residual 1e-10; shape from KUQCD_BATCH_SHAPE or the tuner): the grouped
+multi-right-hand-side dslash kernels in isolation from the rest of the batched workload.
+
+    KUQCD_BATCH_SHAPE=256,8,4,2,0 python -m kuqcd_b200.dslash_bench --dims 24 24 24 48 --batch-sources 4
 """
 from __future__ import annotations
 
@@ -21,6 +27,32 @@ PRECS = {"double": K.KUQCD_DOUBLE, "single": K.KUQCD_SINGLE, "half": K.KUQCD_HAL
 BYTES = {K.KUQCD_DOUBLE: 2400, K.KUQCD_SINGLE: 1200, K.KUQCD_HALF: 608}
 
 
+def batch_sources(ctx, dims, n):
+    """n seeded sources (parity 0, mass 0.03, 12 shifts 1e-4..1) solved together by kq_batch_solve."""
+    Vh = int(np.prod(dims)) // 2
+    vb = ctx.spinor_bytes(K.KUQCD_DOUBLE)
+    sig = list(0.03 ** 2 + np.logspace(-4, 0, 12))
+    batch = K.Batch()
+    keep = []
+    for s in range(n):
+        db = torch.empty(Vh * 6, dtype=torch.float64, device="cuda")
+        ctx.make_source(0, 100 + s, db)
+        d_b = torch.empty(vb, dtype=torch.uint8, device="cuda")
+        ctx.upload(K.KUQCD_DOUBLE, db.cpu().numpy(), d_b)
+        d_x = torch.empty(vb * len(sig), dtype=torch.uint8, device="cuda")
+        batch.add(ctx, d_b, d_x, sig, solver=K.KQ_SOLVER_MIXED, prec=K.KUQCD_HALF, rel_residual=1e-10)
+        keep.append((d_b, d_x))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    info = batch.solve()
+    t = time.perf_counter() - t0
+    print(json.dumps({"dims": list(dims), "batch_sources": n, "seconds": t,
+                      "batched_ms": info.batched_seconds * 1e3, "iterations": info.iterations,
+                      "shape": [info.tile, info.ctas_per_sm, info.rhs_per_cta, info.sites_per_thread,
+                                info.fp64_rhs_per_pass], "max_true_residual": info.max_true_residual}))
+    batch.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--dims", type=int, nargs=4, default=[32, 32, 32, 32])
@@ -29,6 +61,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--eps", type=float, default=0.3)
     ap.add_argument("--ptc", action="store_true", help="time the learned preconditioner's application instead")
+    ap.add_argument("--batch-sources", type=int, default=0,
+                    help="solve this many sources on the field with kq_batch_solve instead")
     args = ap.parse_args()
     dims = tuple(args.dims)
     V = int(np.prod(dims))
@@ -40,6 +74,9 @@ def main():
     ctx.load_links(K.KUQCD_FAT_LINK, dfat.cpu().numpy())
     ctx.load_links(K.KUQCD_LONG_LINK, dlng.cpu().numpy())
     del dfat, dlng
+    if args.batch_sources > 0:
+        batch_sources(ctx, dims, args.batch_sources)
+        return
     db = torch.empty(Vh * 6, dtype=torch.float64, device="cuda")
     ctx.make_source(1, 2, db)
     hb = db.cpu().numpy()

@@ -33,6 +33,7 @@ KUQCD_WILSON_DIRAC, KUQCD_WILSONPC_DIRAC, KUQCD_HISQ_DIRAC, KUQCD_HISQPC_DIRAC =
 KUQCD_CG, KUQCD_CGM = 0, 1
 KQ_SOLVER_CGM, KQ_SOLVER_MIXED, KQ_SOLVER_CGM_WINDOWED = 0, 1, 2
 KQ_PARITY_FULL = 2  # full-lattice (KUQCD_HISQ_DIRAC) fields: parity 0 then parity 1
+KQ_CGM_START, KQ_CGM_ALPHA, KQ_CGM_BETA, KQ_CGM_FINISH = 0, 1, 2, 3  # kq_slab_cgm_step
 
 
 class KuQCDGaugeParam(C.Structure):
@@ -66,7 +67,8 @@ EXPORTED_SYMBOLS = [
     "kq_mdagm_noalloc", "kq_dslash_full", "kq_mdagm_full", "kq_long_links_compressed", "kq_slab_set",
     "kq_slab_face_bytes", "kq_slab_pack_faces", "kq_slab_link_face_bytes", "kq_slab_pack_link_face", "kq_slab_set_link_ghosts",
     "kq_slab_dslash", "kq_slab_dslash_part", "kq_field_axpby", "kq_field_dot", "kq_field_dot_device",
-    "kq_field_ms_update", "kq_host_alloc", "kq_host_free", "kq_apply_host",
+    "kq_field_ms_update", "kq_slab_cgm_state_bytes", "kq_slab_cgm_init", "kq_slab_cgm_step",
+    "kq_slab_cgm_residual", "kq_slab_cgm_update", "kq_slab_cgm_poll", "kq_host_alloc", "kq_host_free", "kq_apply_host",
     "kq_vec_axpby", "kq_vec_dot",
     "kq_solve_multishift", "kq_solve_multishift_device", "kq_true_residuals", "kq_make_links_record",
     "kq_make_source_record", "kq_last_error", "kq_batch_create", "kq_batch_destroy", "kq_batch_add",
@@ -138,6 +140,12 @@ def library() -> C.CDLL:
         "kq_slab_dslash_part": (i, [vp, i, vp, vp, vp, vp, i, vp, d, i, vp]),
         "kq_field_dot_device": (i, [vp, vp, vp, vp, vp]),
         "kq_field_ms_update": (i, [vp, i, C.POINTER(d), C.POINTER(d), C.POINTER(d), vp, vp, vp, sz, vp]),
+        "kq_slab_cgm_state_bytes": (sz, []),
+        "kq_slab_cgm_init": (i, [vp, vp, i, C.POINTER(d), d, i, vp]),
+        "kq_slab_cgm_step": (i, [vp, vp, i, vp]),
+        "kq_slab_cgm_residual": (i, [vp, vp, vp, vp, vp]),
+        "kq_slab_cgm_update": (i, [vp, vp, vp, vp, vp, sz, vp]),
+        "kq_slab_cgm_poll": (i, [vp, vp, C.POINTER(i), C.POINTER(i), vp]),
         "kq_solve_multishift": (i, [vp, C.POINTER(SolveParam), vp, C.POINTER(vp), C.POINTER(SolveInfo)]),
         "kq_solve_multishift_device": (i, [vp, C.POINTER(SolveParam), vp, vp, C.POINTER(SolveInfo)]),
         "kq_true_residuals": (i, [vp, i, i, C.POINTER(d), vp, vp, C.POINTER(d)]),

@@ -80,6 +80,12 @@ class LocalTransport:
         """Sum of the ranks' device tensors, returned on the host (one synchronisation)."""
         return torch.stack([t for t in tensors]).sum(0).cpu().numpy()
 
+    def allreduce_inplace(self, tensors):
+        """Every rank's device tensor becomes the sum over ranks, in stream order (no host synchronisation)."""
+        tot = torch.stack([t.to(tensors[0].device) for t in tensors]).sum(0)
+        for t in tensors:
+            t.copy_(tot)
+
 
 class TorchTransport:
     """One rank per process over torch.distributed (the process group must exist)."""
@@ -123,9 +129,7 @@ class TorchTransport:
         ops = [d.P2POp(d.isend, lo, self._peer(-1), self.group), d.P2POp(d.irecv, ghost_hi, self._peer(1), self.group)]
         for w in d.batch_isend_irecv(ops):
             w.wait()
-        if ghost_lo.is_cuda:
-            # NCCL completion orders only torch's current stream: the slab kernels run on the context's stream
-            torch.cuda.synchronize()
+        # on CUDA, wait() orders torch's current stream after the transfers, and the slab kernels run on that stream
         return [(ghost_lo, ghost_hi)]
 
     def allreduce(self, values):
@@ -141,10 +145,19 @@ class TorchTransport:
         (t,) = tensors
         if self.dist.get_backend(self.group) != "nccl":
             t = t.cpu()
-        else:
-            torch.cuda.synchronize()  # the local sums were written on the context's stream
         self.dist.all_reduce(t, group=self.group)
         return t.cpu().numpy()
+
+    def allreduce_inplace(self, tensors):
+        """This rank's tensor becomes the sum over ranks: NCCL on the device in stream order (no host
+        synchronisation); gloo through the host."""
+        (t,) = tensors
+        if self.dist.get_backend(self.group) == "nccl":
+            self.dist.all_reduce(t, group=self.group)
+        else:
+            h = t.cpu()
+            self.dist.all_reduce(h, group=self.group)
+            t.copy_(h)
 
 
 # ---------------------------------------------------------------------------------------------------- one slab
@@ -162,6 +175,11 @@ class Slab:
         self.ctx = L.Context(self.dims, device)
         self.ctx._chk(L.library().kq_slab_set(self.ctx._h, rank, nranks), "kq_slab_set")
         self._faces = {}
+
+    def stream(self):
+        """torch's current stream on the slab's device: every slab operation, the transport's NCCL calls and the
+        caller's tensor operations are ordered on it, so no step needs a host synchronisation"""
+        return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
 
     def field(self, prec=L.KUQCD_DOUBLE):
         return torch.zeros(self.ctx.spinor_bytes(prec), dtype=torch.uint8, device=f"cuda:{self.device}")
@@ -186,18 +204,19 @@ class Slab:
             self._faces[prec] = tuple(torch.empty(n, dtype=torch.uint8, device=f"cuda:{self.device}")
                                       for _ in range(2))
         lo, hi = self._faces[prec]
-        self.ctx._chk(L.library().kq_slab_pack_faces(self.ctx._h, prec, _p(src), _p(lo), _p(hi), None),
+        self.ctx._chk(L.library().kq_slab_pack_faces(self.ctx._h, prec, _p(src), _p(lo), _p(hi), self.stream()),
                       "kq_slab_pack_faces")
         return lo, hi
 
     def dslash(self, prec, src, ghost_lo, ghost_hi, dst, dst_parity, pvec=None, sigma=0.0, part=PART_ALL):
         self.ctx._chk(L.library().kq_slab_dslash_part(self.ctx._h, prec, _p(src), _p(ghost_lo), _p(ghost_hi),
-                                                      _p(dst), dst_parity, _p(pvec), float(sigma), part, None),
+                                                      _p(dst), dst_parity, _p(pvec), float(sigma), part,
+                                                      self.stream()),
                       "kq_slab_dslash_part")
 
     def dot_device(self, x, y, out):
         """local <x, y> into out (a one-element float64 device tensor), without a host round trip"""
-        self.ctx._chk(L.library().kq_field_dot_device(self.ctx._h, _p(x), _p(y), _p(out), None),
+        self.ctx._chk(L.library().kq_field_dot_device(self.ctx._h, _p(x), _p(y), _p(out), self.stream()),
                       "kq_field_dot_device")
 
     def ms_update(self, B, Z, a, r, p_block, x_block, n):
@@ -205,12 +224,44 @@ class Slab:
         vb = self.ctx.spinor_bytes(L.KUQCD_DOUBLE)
         arr = [np.ascontiguousarray(v[:max(n, 1)], dtype=np.float64) for v in (B, Z, a)]
         ptr = [v.ctypes.data_as(C.POINTER(C.c_double)) for v in arr]
-        self.ctx._chk(L.library().kq_field_ms_update(self.ctx._h, n, *ptr, _p(r), _p(p_block), _p(x_block), vb, None),
+        self.ctx._chk(L.library().kq_field_ms_update(self.ctx._h, n, *ptr, _p(r), _p(p_block), _p(x_block), vb,
+                                                     self.stream()),
                       "kq_field_ms_update")
 
     def axpby(self, a, x, b, y):
-        self.ctx._chk(L.library().kq_field_axpby(self.ctx._h, float(a), _p(x), float(b), _p(y), None),
+        self.ctx._chk(L.library().kq_field_axpby(self.ctx._h, float(a), _p(x), float(b), _p(y), self.stream()),
                       "kq_field_axpby")
+
+    # device-driven multishift CG (kq_slab_cgm_*): the state is a float64 device tensor whose first two elements are
+    # the sums the transport all-reduces in place
+    def cgm_state(self):
+        n = L.library().kq_slab_cgm_state_bytes()
+        return torch.zeros(n // 8, dtype=torch.float64, device=f"cuda:{self.device}")
+
+    def cgm_init(self, state, shifts_ref, tol, max_iter):
+        sh = np.ascontiguousarray(shifts_ref, dtype=np.float64)
+        self.ctx._chk(L.library().kq_slab_cgm_init(self.ctx._h, _p(state), len(sh),
+                                                   sh.ctypes.data_as(C.POINTER(C.c_double)), float(tol),
+                                                   int(max_iter), self.stream()), "kq_slab_cgm_init")
+
+    def cgm_step(self, state, step):
+        self.ctx._chk(L.library().kq_slab_cgm_step(self.ctx._h, _p(state), step, self.stream()), "kq_slab_cgm_step")
+
+    def cgm_residual(self, state, s, r):
+        self.ctx._chk(L.library().kq_slab_cgm_residual(self.ctx._h, _p(state), _p(s), _p(r), self.stream()),
+                      "kq_slab_cgm_residual")
+
+    def cgm_update(self, state, r, p_block, x_block):
+        vb = self.ctx.spinor_bytes(L.KUQCD_DOUBLE)
+        self.ctx._chk(L.library().kq_slab_cgm_update(self.ctx._h, _p(state), _p(r), _p(p_block), _p(x_block), vb,
+                                                     self.stream()), "kq_slab_cgm_update")
+
+    def cgm_poll(self, state):
+        """(iterations, stopped) of the state; waits for the stream"""
+        it, done = C.c_int(), C.c_int()
+        self.ctx._chk(L.library().kq_slab_cgm_poll(self.ctx._h, _p(state), C.byref(it), C.byref(done),
+                                                   self.stream()), "kq_slab_cgm_poll")
+        return it.value, bool(done.value)
 
     def dot(self, x, y) -> float:
         out = C.c_double()
@@ -236,7 +287,7 @@ def dslash(slabs, transport, prec, srcs, dsts, dst_parity, pvecs=None, sigma=0.0
     interior sites (which read no ghost) are computed while the faces are in flight, the boundary sites after they
     have arrived -- the reference's StartComm / bulk loop / EndComm (dirac_hisq.cpp:412-414, 452-454)."""
     faces = [s.pack(prec, x) for s, x in zip(slabs, srcs)]
-    torch.cuda.synchronize()  # faces packed before the transport reads them
+    # packs, transfers and kernels are ordered on torch's current stream: no host synchronisation
     handle = transport.exchange_start(faces)
     pv = [None if pvecs is None else pvecs[k] for k in range(len(slabs))]
     if overlap:
@@ -245,29 +296,20 @@ def dslash(slabs, transport, prec, srcs, dsts, dst_parity, pvecs=None, sigma=0.0
     ghosts = transport.exchange_wait(handle)
     for k, (s, x, y, (glo, ghi)) in enumerate(zip(slabs, srcs, dsts, ghosts)):
         s.dslash(prec, x, glo, ghi, y, dst_parity, pv[k], sigma, part=PART_BOUNDARY if overlap else PART_ALL)
-    torch.cuda.synchronize()
 
 
-def cgm(slabs, transport, bs, shifts_ref, tol, max_iter, parity=0, overlap=True):
+def cgm(slabs, transport, bs, shifts_ref, tol, max_iter, parity=0, overlap=True, poll_every=4):
     """Multishift CG of inverter_cgm.cpp:17-87 on FP64 slab fields.  shifts_ref: reference semantics (x_0 solves
     shifts[0] - DD, x_j solves shifts[0] + shifts[j] - DD); stops shift k when Z_k^2 |r|^2 < tol.  Returns
     (xs, iterations) with xs[r][k] the local solution of shift k on slab r.
 
-    Per iteration: two dslash with overlapped halo exchange, two reductions -- each a device-side local sum and one
-    all-reduce over ranks (the reference's MPI_Allreduce, spinor_field.cpp:207-215, 235-243) -- the shifted scalar
-    recurrences vectorised over the shifts, and one fused pass over all shift vectors (kq_field_ms_update)."""
+    Device-driven: the scalar recurrences run on a device state (kq_slab_cgm_*), each of the two reductions per
+    iteration is a device-side local sum and one in-place all-reduce over ranks (the reference's MPI_Allreduce,
+    spinor_field.cpp:207-215, 235-243), the shift vectors are updated in one fused pass, and the two dslash overlap
+    their halo exchange; everything is ordered on torch's current stream.  The host reads the state once every
+    poll_every iterations (steps after the stop are no-ops, so the iteration count is the reference's)."""
     ns = len(shifts_ref)
     D = L.KUQCD_DOUBLE
-    sh = np.asarray(shifts_ref, dtype=np.float64)
-
-    def allsum(x, y):
-        outs = []
-        for s, xk, yk in zip(slabs, x, y):
-            o = torch.zeros(1, dtype=torch.float64, device=f"cuda:{s.device}")
-            s.dot_device(xk, yk, o)
-            outs.append(o)
-        return float(transport.allreduce_device(outs)[0])
-
     vb = [s.ctx.spinor_bytes(D) for s in slabs]
     r = [s.field() for s in slabs]
     sv = [s.field() for s in slabs]
@@ -275,42 +317,34 @@ def cgm(slabs, transport, bs, shifts_ref, tol, max_iter, parity=0, overlap=True)
     pblk = [torch.zeros(ns * n, dtype=torch.uint8, device=f"cuda:{s.device}") for s, n in zip(slabs, vb)]
     xblk = [torch.zeros(ns * n, dtype=torch.uint8, device=f"cuda:{s.device}") for s, n in zip(slabs, vb)]
     p0 = [pb[:n] for pb, n in zip(pblk, vb)]
+    st = [s.cgm_state() for s in slabs]
     for k, s in enumerate(slabs):
+        s.cgm_init(st[k], shifts_ref, tol, max_iter)
         s.axpby(1.0, bs[k], 0.0, r[k])
         for j in range(ns):
             s.axpby(1.0, bs[k], 0.0, pblk[k][j * vb[k]:(j + 1) * vb[k]])
-    a = np.zeros(ns)
-    B = np.ones(ns)
-    Z = np.ones(ns)
-    Zm1 = np.ones(ns)
-    rr = allsum(r, r)
-    Bm1, max_term, it = 1.0, ns, 0
-    while True:
-        it += 1
-        # s = shifts[0] p0 - D_pq D_qp p0 (MdaggM + Axmy, inverter_cgm.cpp:44-46)
-        dslash(slabs, transport, D, p0, tmp, 1 - parity, overlap=overlap)
-        dslash(slabs, transport, D, tmp, sv, parity, pvecs=p0, sigma=shifts_ref[0], overlap=overlap)
-        pAp = allsum(p0, sv)
-        B[0] = -rr / pAp
-        for k, s in enumerate(slabs):
-            s.axpby(B[0], sv[k], 1.0, r[k])
-        j = slice(1, max_term)
-        rr1 = Bm1 * Zm1[j] / (B[0] * a[0] * (Zm1[j] - Z[j]) + Zm1[j] * Bm1 * (1.0 - sh[j] * B[0]))
-        Zm1[j] = Z[j]
-        Z[j] = Z[j] * rr1
-        B[j] = B[0] * rr1
-        Bm1 = B[0]
-        lam2 = allsum(r, r)
-        a[0] = lam2 / rr
-        rr = lam2
-        a[j] = a[0] * Z[j] * B[j] / (Zm1[j] * B[0])
-        # x_j -= B_j p_j ; p_j = Z_j r + a_j p_j  (Z_0 = 1), all shifts in one pass
-        for k, s in enumerate(slabs):
-            s.ms_update(B, Z, a, r[k], pblk[k], xblk[k], max_term)
-        while max_term > 0 and Z[max_term - 1] ** 2 * lam2 < tol:
-            max_term -= 1
-        if max_term == 0 or it >= max_iter:
-            break
+        s.dot_device(r[k], r[k], st[k][1:2])
+    transport.allreduce_inplace([t[1:2] for t in st])
+    for k, s in enumerate(slabs):
+        s.cgm_step(st[k], L.KQ_CGM_START)
+    it, done = slabs[0].cgm_poll(st[0])
+    while not done:
+        for _ in range(poll_every):
+            # s = shifts[0] p0 - D_pq D_qp p0 (MdaggM + Axmy, inverter_cgm.cpp:44-46)
+            dslash(slabs, transport, D, p0, tmp, 1 - parity, overlap=overlap)
+            dslash(slabs, transport, D, tmp, sv, parity, pvecs=p0, sigma=shifts_ref[0], overlap=overlap)
+            for k, s in enumerate(slabs):
+                s.dot_device(p0[k], sv[k], st[k][0:1])
+            transport.allreduce_inplace([t[0:1] for t in st])
+            for k, s in enumerate(slabs):
+                s.cgm_step(st[k], L.KQ_CGM_ALPHA)
+                s.cgm_residual(st[k], sv[k], r[k])
+            transport.allreduce_inplace([t[1:2] for t in st])
+            for k, s in enumerate(slabs):
+                s.cgm_step(st[k], L.KQ_CGM_BETA)
+                s.cgm_update(st[k], r[k], pblk[k], xblk[k])
+                s.cgm_step(st[k], L.KQ_CGM_FINISH)
+        it, done = slabs[0].cgm_poll(st[0])
     torch.cuda.synchronize()
     x = [[xblk[k][j * vb[k]:(j + 1) * vb[k]] for j in range(ns)] for k in range(len(slabs))]
     return x, it

@@ -84,8 +84,11 @@ def test_slab_sigma_minus_dslash_and_operator(cuda):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("R", [2, 4])
-def test_slab_multishift_cg_solves_global_system(cuda, R):
+@pytest.mark.parametrize("R,poll_every", [(2, 1), (2, 5), (4, 4)])
+def test_slab_multishift_cg_solves_global_system(cuda, R, poll_every):
+    """The device-driven slab CGM (scalar recurrences on a device state, in-place reductions, host poll every few
+    iterations) solves the global system with the reference's recurrences; steps after the stop are no-ops, so the
+    iteration count does not depend on the poll interval."""
     slabs, tr, fat, lng = setup_slabs(R, 0.3, 11)
     b = O.make_source(GDIMS, 0, 8)
     m, sig = 0.05, np.logspace(-3, 0, 5)
@@ -93,7 +96,7 @@ def test_slab_multishift_cg_solves_global_system(cuda, R):
     refsh = [ab[0]] + list(sig[1:] - sig[0])
     tol = (1e-10) ** 2 * float(b @ b)
     bs = upload(slabs, b)
-    xs, it = SL.cgm(slabs, tr, bs, refsh, tol, 5000)
+    xs, it = SL.cgm(slabs, tr, bs, refsh, tol, 5000, poll_every=poll_every)
     xo, ito = O.cgm(GDIMS, fat, lng, 0, refsh, b, tol, 5000)
     assert abs(it - ito) <= 1, (it, ito)  # same recurrences; reductions summed in another order
     for k in range(len(ab)):
@@ -130,3 +133,16 @@ def test_slab_dslash_parts_and_half(cuda, R):
         got, whole = download(slabs, ys, prec), download(slabs, zs, prec)
         assert np.array_equal(got, whole), prec
         assert np.linalg.norm(got - want) <= tol * np.linalg.norm(want), prec
+
+
+@pytest.mark.gpu
+def test_slab_cgm_zero_source_and_iteration_cap(cuda):
+    """b = 0 stops before the first iteration with x = 0; max_iter caps the device-side count exactly."""
+    slabs, tr, fat, lng = setup_slabs(2, 0.3, 12)
+    zero = upload(slabs, np.zeros(GDIMS[0] * GDIMS[1] * GDIMS[2] * GDIMS[3] // 2 * 6))
+    xs, it = SL.cgm(slabs, tr, zero, [0.01, 0.1], 1e-20, 50)
+    assert it == 0
+    assert not np.any(download(slabs, [xk[0] for xk in xs]))
+    b = O.make_source(GDIMS, 0, 9)
+    xs, it = SL.cgm(slabs, tr, upload(slabs, b), [0.0025, 0.1], 1e-40, 7, poll_every=3)
+    assert it == 7

@@ -44,7 +44,11 @@ def _exchange_worker(rank, world, port, out_dir):
         hi = torch.from_numpy(np.ascontiguousarray(loc[(lt - 3) * S:]))    # slices lt-3..lt-1
         (glo, ghi), = tr.exchange([(lo, hi)])
         red = tr.allreduce([np.array([rank + 1.0, 2.0 ** rank])])[0]
-        np.savez(os.path.join(out_dir, f"r{rank}.npz"), glo=glo.numpy(), ghi=ghi.numpy(), red=red)
+        # the device-driven solver's in-place reduction of one slice of a state tensor
+        state = torch.tensor([rank + 1.0, 10.0 * rank, -1.0], dtype=torch.float64)
+        tr.allreduce_inplace([state[1:2]])
+        np.savez(os.path.join(out_dir, f"r{rank}.npz"), glo=glo.numpy(), ghi=ghi.numpy(), red=red,
+                 state=state.numpy())
     finally:
         dist.destroy_process_group()
 
@@ -63,6 +67,7 @@ def test_slab_halo_exchange_gloo(tmp_path, world):
         assert np.array_equal(z["glo"], want_lo), r
         assert np.array_equal(z["ghi"], want_hi), r
         assert np.allclose(z["red"], [world * (world + 1) / 2, 2.0 ** world - 1])
+        assert np.array_equal(z["state"], [r + 1.0, 10.0 * world * (world - 1) / 2, -1.0])
 
 
 def test_slab_record_slicing_round_trip():
@@ -83,6 +88,9 @@ def test_local_transport_is_periodic_ring():
     faces = [(f"lo{r}", f"hi{r}") for r in range(4)]
     assert tr.exchange(faces) == [("hi3", "lo1"), ("hi0", "lo2"), ("hi1", "lo3"), ("hi2", "lo0")]
     assert [list(v) for v in tr.allreduce([[1.0, 2.0], [3.0, 4.0]])] == [[4.0, 6.0], [4.0, 6.0]]
+    st = [torch.tensor([1.0, 2.0, 3.0], dtype=torch.float64), torch.tensor([4.0, 5.0, 6.0], dtype=torch.float64)]
+    tr.allreduce_inplace([t[0:2] for t in st])
+    assert [t.tolist() for t in st] == [[5.0, 7.0, 3.0], [5.0, 7.0, 6.0]]
 
 
 @pytest.mark.skipif(not O.ref_available(), reason="reference library not built here")
