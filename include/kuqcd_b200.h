@@ -185,8 +185,9 @@ KuQCDStatus kq_slab_cgm_residual(kq_context *ctx, kq_slab_cgm_state *d_state, co
                                  void *stream);
 KuQCDStatus kq_slab_cgm_update(kq_context *ctx, const kq_slab_cgm_state *d_state, const void *d_r, void *d_p,
                                void *d_x, size_t stride, void *stream);
-/* iterations so far and whether the solve has stopped (waits for the stream) */
-KuQCDStatus kq_slab_cgm_poll(kq_context *ctx, const kq_slab_cgm_state *d_state, int *iter, int *done, void *stream);
+/* iterations so far, whether the solve has stopped and (rr != NULL) the current |r|^2 (waits for the stream) */
+KuQCDStatus kq_slab_cgm_poll(kq_context *ctx, const kq_slab_cgm_state *d_state, int *iter, int *done, double *rr,
+                             void *stream);
 
 /* ---------------------------------------------------------------- solver */
 enum {

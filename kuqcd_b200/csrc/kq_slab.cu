@@ -574,14 +574,17 @@ __global__ void slab_cgm_step_kernel(kq_slab_cgm_state *st, int step)
             if (!(st->rr > 0.0) || !isfinite(st->rr)) st->done = 1;
         }
     } else if (step == KQ_CGM_ALPHA) {
-        // B_0 = -|r|^2 / <p, A p>; the shifted B_j, Z_j with the previous a_0 and B_0 (inverter_cgm.cpp:47-57)
+        // B_0 = -|r|^2 / <p, A p>; the shifted B_j, Z_j with the previous a_0 and B_0 (inverter_cgm.cpp:47-57).
+        // Every product and sum rounded on its own (no FMA contraction), as a host evaluates the same expressions.
         const double B0 = -st->rr / st->sums[0], a0 = st->a[0], Bm1 = st->Bm1;
         if (j >= 1 && j < st->max_term) {
             const double z = st->Z[j], zm1 = st->Zm1[j];
-            const double rr1 = Bm1 * zm1 / (B0 * a0 * (zm1 - z) + zm1 * Bm1 * (1.0 - st->sh[j] * B0));
+            const double den = __dadd_rn(__dmul_rn(__dmul_rn(B0, a0), __dsub_rn(zm1, z)),
+                                         __dmul_rn(__dmul_rn(zm1, Bm1), __dsub_rn(1.0, __dmul_rn(st->sh[j], B0))));
+            const double rr1 = __dmul_rn(Bm1, zm1) / den;
             st->Zm1[j] = z;
-            st->Z[j] = z * rr1;
-            st->B[j] = B0 * rr1;
+            st->Z[j] = __dmul_rn(z, rr1);
+            st->B[j] = __dmul_rn(B0, rr1);
         }
         __syncthreads();
         if (j == 0) {
@@ -591,7 +594,8 @@ __global__ void slab_cgm_step_kernel(kq_slab_cgm_state *st, int step)
     } else if (step == KQ_CGM_BETA) {
         // a_0 = |r_new|^2 / |r|^2 and the shifted a_j (inverter_cgm.cpp:58-66)
         const double lam2 = st->sums[1], a0 = lam2 / st->rr, B0 = st->B[0];
-        if (j >= 1 && j < st->max_term) st->a[j] = a0 * st->Z[j] * st->B[j] / (st->Zm1[j] * B0);
+        if (j >= 1 && j < st->max_term)
+            st->a[j] = __dmul_rn(__dmul_rn(a0, st->Z[j]), st->B[j]) / __dmul_rn(st->Zm1[j], B0);
         __syncthreads();
         if (j == 0) {
             st->a[0] = a0;
@@ -599,7 +603,7 @@ __global__ void slab_cgm_step_kernel(kq_slab_cgm_state *st, int step)
         }
     } else if (j == 0) {  // KQ_CGM_FINISH: drop converged shifts from the end (inverter_cgm.cpp:70-80)
         int mt = st->max_term;
-        while (mt > 0 && st->Z[mt - 1] * st->Z[mt - 1] * st->rr < st->tol) --mt;
+        while (mt > 0 && __dmul_rn(__dmul_rn(st->Z[mt - 1], st->Z[mt - 1]), st->rr) < st->tol) --mt;
         st->max_term = mt;
         st->iter += 1;
         st->done = (mt == 0 || st->iter >= st->max_iter) ? 1 : 0;
@@ -727,19 +731,20 @@ KQ_API KuQCDStatus kq_slab_cgm_update(kq_context *ctx, const kq_slab_cgm_state *
 }
 
 KQ_API KuQCDStatus kq_slab_cgm_poll(kq_context *ctx, const kq_slab_cgm_state *d_state, int *iter, int *done,
-                                    void *stream)
+                                    double *rr, void *stream)
 {
     if (!ctx || !d_state || !iter || !done) return KUQCD_ERR_NULL_POINTER;
     cudaSetDevice(ctx->device);
-    int h[5] = {0, 0, 0, 0, 0};  // iter, max_iter, num_shift, max_term, done
+    kq_slab_cgm_state h;  // the scalar head: sums, rr, Bm1, tol and the counters
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
-    cudaError_t e = cudaMemcpyAsync(h, &d_state->iter, sizeof(h), cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaMemcpyAsync(&h, d_state, offsetof(kq_slab_cgm_state, sh), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         set_last_error(std::string("kq_slab_cgm_poll: ") + cudaGetErrorString(e));
         return status_of(e);
     }
-    *iter = h[0];
-    *done = h[4];
+    *iter = h.iter;
+    *done = h.done;
+    if (rr) *rr = h.rr;
     return KUQCD_SUCCESS;
 }

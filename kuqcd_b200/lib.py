@@ -145,7 +145,7 @@ def library() -> C.CDLL:
         "kq_slab_cgm_step": (i, [vp, vp, i, vp]),
         "kq_slab_cgm_residual": (i, [vp, vp, vp, vp, vp]),
         "kq_slab_cgm_update": (i, [vp, vp, vp, vp, vp, sz, vp]),
-        "kq_slab_cgm_poll": (i, [vp, vp, C.POINTER(i), C.POINTER(i), vp]),
+        "kq_slab_cgm_poll": (i, [vp, vp, C.POINTER(i), C.POINTER(i), C.POINTER(d), vp]),
         "kq_solve_multishift": (i, [vp, C.POINTER(SolveParam), vp, C.POINTER(vp), C.POINTER(SolveInfo)]),
         "kq_solve_multishift_device": (i, [vp, C.POINTER(SolveParam), vp, vp, C.POINTER(SolveInfo)]),
         "kq_true_residuals": (i, [vp, i, i, C.POINTER(d), vp, vp, C.POINTER(d)]),
@@ -223,6 +223,28 @@ def kuqcd_end() -> None:
 
 
 # ---------------------------------------------------------------- device-level API
+# Device buffers usually come from torch, whose kernels (a torch.zeros fill, a copy) run on torch's current stream,
+# while a context's own stream is non-blocking.  So the calls below run on torch's current stream unless given one,
+# and the calls that only use the library's own streams first wait for torch's pending work on the device.  Every
+# call returns with its results complete, or enqueued on torch's stream.
+CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy: the legacy default stream, by a handle that is not NULL
+
+
+def _torch_stream(device: int):
+    """torch's current stream on `device` as a library stream argument.  torch's default stream has the handle 0,
+    which the library would read as 'the context's own stream', so it is passed as cudaStreamLegacy."""
+    import torch
+
+    h = torch.cuda.current_stream(device).cuda_stream
+    return C.c_void_p(h if h else CUDA_STREAM_LEGACY)
+
+
+def _torch_wait(device: int):
+    import torch
+
+    torch.cuda.current_stream(device).synchronize()
+
+
 class Context:
     """One lattice on one GPU (kq_context): device links, stream, solver workspace."""
 
@@ -236,6 +258,10 @@ class Context:
         if st != 0:
             raise KuQCDError(st, "kq_context_create")
         self._h = h
+        self.device = device
+
+    def _s(self, stream):
+        return stream if stream is not None else _torch_stream(self.device)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -265,29 +291,29 @@ class Context:
 
     def upload(self, prec: int, host: np.ndarray, dev, stream=None):
         host = np.ascontiguousarray(host)
-        self._chk(library().kq_spinor_upload(self._h, prec, _ptr(host), _np_prec(host), _ptr(dev), stream),
+        self._chk(library().kq_spinor_upload(self._h, prec, _ptr(host), _np_prec(host), _ptr(dev), self._s(stream)),
                   "kq_spinor_upload")
 
     def download(self, prec: int, dev, host_dtype=np.float64, stream=None) -> np.ndarray:
         out = np.empty(self.Vh * 6, dtype=host_dtype)
-        self._chk(library().kq_spinor_download(self._h, prec, _ptr(dev), _ptr(out), _np_prec(out), stream),
+        self._chk(library().kq_spinor_download(self._h, prec, _ptr(dev), _ptr(out), _np_prec(out), self._s(stream)),
                   "kq_spinor_download")
         return out
 
     def convert(self, src, src_prec: int, dst, dst_prec: int, stream=None):
-        self._chk(library().kq_spinor_convert(self._h, _ptr(src), src_prec, _ptr(dst), dst_prec, stream),
+        self._chk(library().kq_spinor_convert(self._h, _ptr(src), src_prec, _ptr(dst), dst_prec, self._s(stream)),
                   "kq_spinor_convert")
 
     def dslash(self, prec: int, src, dst, dst_parity: int, stream=None):
-        self._chk(library().kq_dslash(self._h, prec, _ptr(src), _ptr(dst), dst_parity, stream), "kq_dslash")
+        self._chk(library().kq_dslash(self._h, prec, _ptr(src), _ptr(dst), dst_parity, self._s(stream)), "kq_dslash")
 
     def mdagm(self, prec: int, sigma: float, src, dst, tmp, parity: int, stream=None):
-        self._chk(library().kq_mdagm(self._h, prec, sigma, _ptr(src), _ptr(dst), _ptr(tmp), parity, stream),
+        self._chk(library().kq_mdagm(self._h, prec, sigma, _ptr(src), _ptr(dst), _ptr(tmp), parity, self._s(stream)),
                   "kq_mdagm")
 
     def mdagm_noalloc(self, prec: int, sigma: float, src, dst, parity: int, stream=None) -> int:
         """kq_mdagm_noalloc: returns the status (callers test the rejection paths)."""
-        return library().kq_mdagm_noalloc(self._h, prec, sigma, _ptr(src), _ptr(dst), parity, stream)
+        return library().kq_mdagm_noalloc(self._h, prec, sigma, _ptr(src), _ptr(dst), parity, self._s(stream))
 
     def long_links_compressed(self, prec: int) -> int:
         """1: long links of prec stored as two rows + 1/s; 0: full storage; -1: not resident."""
@@ -310,10 +336,10 @@ class Context:
 
     def dslash_full(self, prec: int, src, dst, stream=None):
         """kq_dslash_full: D on full-lattice fields (both parities, one launch)."""
-        self._chk(library().kq_dslash_full(self._h, prec, _ptr(src), _ptr(dst), stream), "kq_dslash_full")
+        self._chk(library().kq_dslash_full(self._h, prec, _ptr(src), _ptr(dst), self._s(stream)), "kq_dslash_full")
 
     def mdagm_full(self, prec: int, sigma: float, src, dst, tmp, stream=None):
-        self._chk(library().kq_mdagm_full(self._h, prec, sigma, _ptr(src), _ptr(dst), _ptr(tmp), stream),
+        self._chk(library().kq_mdagm_full(self._h, prec, sigma, _ptr(src), _ptr(dst), _ptr(tmp), self._s(stream)),
                   "kq_mdagm_full")
 
     @staticmethod
@@ -350,6 +376,7 @@ class Context:
                      tol=0.0, rel_residual=1e-10, shift_mode=1):
         p, keep = self._param(shifts, parity, solver, prec, KUQCD_DOUBLE, max_iter, tol, rel_residual, shift_mode)
         info = SolveInfo()
+        _torch_wait(self.device)
         self._chk(library().kq_solve_multishift_device(self._h, C.byref(p), _ptr(d_b), _ptr(d_x), C.byref(info)),
                   "kq_solve_multishift_device")
         return info
@@ -357,15 +384,18 @@ class Context:
     def true_residuals(self, parity, sigmas, d_b, d_x):
         sg = (C.c_double * len(sigmas))(*[float(s) for s in sigmas])
         out = (C.c_double * len(sigmas))()
+        _torch_wait(self.device)
         self._chk(library().kq_true_residuals(self._h, parity, len(sigmas), sg, _ptr(d_b), _ptr(d_x), out),
                   "kq_true_residuals")
         return list(out)
 
     def make_links(self, eps: float, seed: int, d_fat, d_long):
+        _torch_wait(self.device)
         self._chk(library().kq_make_links_record(self._h, eps, seed, _ptr(d_fat), _ptr(d_long)),
                   "kq_make_links_record")
 
     def make_source(self, parity: int, seed: int, d_b):
+        _torch_wait(self.device)
         self._chk(library().kq_make_source_record(self._h, parity, seed, _ptr(d_b)), "kq_make_source_record")
 
 
@@ -378,6 +408,7 @@ class Batch:
         if st != 0:
             raise KuQCDError(st, "kq_batch_create")
         self._h = h
+        self._device = device
         self._keep = []
 
     def add(self, ctx: Context, d_b, d_x, shifts, parity=0, solver=KQ_SOLVER_MIXED, prec=KUQCD_HALF,
@@ -390,6 +421,7 @@ class Batch:
 
     def solve(self) -> BatchInfo:
         info = BatchInfo()
+        _torch_wait(self._device)
         st = library().kq_batch_solve(self._h, C.byref(info))
         if st != 0:
             raise KuQCDError(st, "kq_batch_solve")
@@ -456,10 +488,12 @@ class Net:
         self.ctx = ctx
 
     def apply(self, d_in, d_out, parity: int):
+        _torch_wait(self.ctx.device)
         self._chk(library().kq_net_apply(self._h, _ptr(d_in), _ptr(d_out), parity), "kq_net_apply")
 
     def train_pair(self, d_r, d_e, parity: int, e_norm2: float) -> float:
         loss = C.c_double()
+        _torch_wait(self.ctx.device)
         self._chk(library().kq_net_train_pair(self._h, _ptr(d_r), _ptr(d_e), parity, e_norm2, C.byref(loss)),
                   "kq_net_train_pair")
         return loss.value
@@ -484,6 +518,7 @@ def fcg_polish(ctx: Context, net, d_b, d_x, shifts, parity=0, rel_residual=1e-10
     p, keep = Context._param(shifts, parity, KQ_SOLVER_MIXED, KUQCD_DOUBLE, KUQCD_DOUBLE, max_iter, 0.0,
                              rel_residual, 1)
     info = SolveInfo()
+    _torch_wait(ctx.device)
     st = library().kq_fcg_polish(ctx._h, net._h if net is not None else None, C.byref(p), _ptr(d_b), _ptr(d_x),
                                  C.byref(info))
     if st != 0:

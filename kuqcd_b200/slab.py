@@ -179,7 +179,7 @@ class Slab:
     def stream(self):
         """torch's current stream on the slab's device: every slab operation, the transport's NCCL calls and the
         caller's tensor operations are ordered on it, so no step needs a host synchronisation"""
-        return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        return L._torch_stream(self.device)
 
     def field(self, prec=L.KUQCD_DOUBLE):
         return torch.zeros(self.ctx.spinor_bytes(prec), dtype=torch.uint8, device=f"cuda:{self.device}")
@@ -256,15 +256,16 @@ class Slab:
         self.ctx._chk(L.library().kq_slab_cgm_update(self.ctx._h, _p(state), _p(r), _p(p_block), _p(x_block), vb,
                                                      self.stream()), "kq_slab_cgm_update")
 
-    def cgm_poll(self, state):
-        """(iterations, stopped) of the state; waits for the stream"""
-        it, done = C.c_int(), C.c_int()
+    def cgm_poll(self, state, with_rr=False):
+        """(iterations, stopped[, |r|^2]) of the state; waits for the stream"""
+        it, done, rr = C.c_int(), C.c_int(), C.c_double()
         self.ctx._chk(L.library().kq_slab_cgm_poll(self.ctx._h, _p(state), C.byref(it), C.byref(done),
-                                                   self.stream()), "kq_slab_cgm_poll")
-        return it.value, bool(done.value)
+                                                   C.byref(rr), self.stream()), "kq_slab_cgm_poll")
+        return (it.value, bool(done.value), rr.value) if with_rr else (it.value, bool(done.value))
 
     def dot(self, x, y) -> float:
         out = C.c_double()
+        L._torch_wait(self.device)  # kq_field_dot runs on the context's stream
         self.ctx._chk(L.library().kq_field_dot(self.ctx._h, _p(x), _p(y), C.byref(out)), "kq_field_dot")
         return out.value
 
@@ -298,16 +299,32 @@ def dslash(slabs, transport, prec, srcs, dsts, dst_parity, pvecs=None, sigma=0.0
         s.dslash(prec, x, glo, ghi, y, dst_parity, pv[k], sigma, part=PART_BOUNDARY if overlap else PART_ALL)
 
 
-def cgm(slabs, transport, bs, shifts_ref, tol, max_iter, parity=0, overlap=True, poll_every=4):
-    """Multishift CG of inverter_cgm.cpp:17-87 on FP64 slab fields.  shifts_ref: reference semantics (x_0 solves
-    shifts[0] - DD, x_j solves shifts[0] + shifts[j] - DD); stops shift k when Z_k^2 |r|^2 < tol.  Returns
-    (xs, iterations) with xs[r][k] the local solution of shift k on slab r.
+def _global_dot(slabs, transport, x, y) -> float:
+    outs = [torch.zeros(1, dtype=torch.float64, device=f"cuda:{s.device}") for s in slabs]
+    for s, xk, yk, o in zip(slabs, x, y, outs):
+        s.dot_device(xk, yk, o)
+    transport.allreduce_inplace(outs)
+    return float(outs[0].item())
 
-    Device-driven: the scalar recurrences run on a device state (kq_slab_cgm_*), each of the two reductions per
-    iteration is a device-side local sum and one in-place all-reduce over ranks (the reference's MPI_Allreduce,
-    spinor_field.cpp:207-215, 235-243), the shift vectors are updated in one fused pass, and the two dslash overlap
-    their halo exchange; everything is ordered on torch's current stream.  The host reads the state once every
-    poll_every iterations (steps after the stop are no-ops, so the iteration count is the reference's)."""
+
+def _operator(slabs, transport, prec, p0, tmp, sv, sloppy, parity, sigma, overlap):
+    """sv = sigma p0 - D_pq D_qp p0 on FP64 slab fields, the dslash in precision prec (p0 converted to it, the result
+    converted back: the inexact matvec of a relaxed-precision Krylov solver)"""
+    D = L.KUQCD_DOUBLE
+    if prec == D:
+        dslash(slabs, transport, D, p0, tmp, 1 - parity, overlap=overlap)
+        dslash(slabs, transport, D, tmp, sv, parity, pvecs=p0, sigma=sigma, overlap=overlap)
+        return
+    ps, ts, ss = sloppy[prec]
+    for k, s in enumerate(slabs):
+        s.ctx.convert(p0[k], D, ps[k], prec, s.stream())
+    dslash(slabs, transport, prec, ps, ts, 1 - parity, overlap=overlap)
+    dslash(slabs, transport, prec, ts, ss, parity, pvecs=ps, sigma=sigma, overlap=overlap)
+    for k, s in enumerate(slabs):
+        s.ctx.convert(ss[k], prec, sv[k], D, s.stream())
+
+
+def _cgm(slabs, transport, bs, shifts_ref, tol, max_iter, parity, overlap, poll_every, choose=None, log=None):
     ns = len(shifts_ref)
     D = L.KUQCD_DOUBLE
     vb = [s.ctx.spinor_bytes(D) for s in slabs]
@@ -327,12 +344,15 @@ def cgm(slabs, transport, bs, shifts_ref, tol, max_iter, parity=0, overlap=True,
     transport.allreduce_inplace([t[1:2] for t in st])
     for k, s in enumerate(slabs):
         s.cgm_step(st[k], L.KQ_CGM_START)
-    it, done = slabs[0].cgm_poll(st[0])
+    it, done, rr = slabs[0].cgm_poll(st[0], with_rr=True)
+    sloppy = {}
     while not done:
+        prec = D if choose is None else choose(rr)
+        if prec != D and prec not in sloppy:
+            sloppy[prec] = tuple([s.field(prec) for s in slabs] for _ in range(3))
         for _ in range(poll_every):
             # s = shifts[0] p0 - D_pq D_qp p0 (MdaggM + Axmy, inverter_cgm.cpp:44-46)
-            dslash(slabs, transport, D, p0, tmp, 1 - parity, overlap=overlap)
-            dslash(slabs, transport, D, tmp, sv, parity, pvecs=p0, sigma=shifts_ref[0], overlap=overlap)
+            _operator(slabs, transport, prec, p0, tmp, sv, sloppy, parity, shifts_ref[0], overlap)
             for k, s in enumerate(slabs):
                 s.dot_device(p0[k], sv[k], st[k][0:1])
             transport.allreduce_inplace([t[0:1] for t in st])
@@ -344,7 +364,72 @@ def cgm(slabs, transport, bs, shifts_ref, tol, max_iter, parity=0, overlap=True,
                 s.cgm_step(st[k], L.KQ_CGM_BETA)
                 s.cgm_update(st[k], r[k], pblk[k], xblk[k])
                 s.cgm_step(st[k], L.KQ_CGM_FINISH)
-        it, done = slabs[0].cgm_poll(st[0])
+        it2, done, rr = slabs[0].cgm_poll(st[0], with_rr=True)
+        if log is not None:
+            log[prec] = log.get(prec, 0) + it2 - it
+        it = it2
     torch.cuda.synchronize()
     x = [[xblk[k][j * vb[k]:(j + 1) * vb[k]] for j in range(ns)] for k in range(len(slabs))]
     return x, it
+
+
+def cgm(slabs, transport, bs, shifts_ref, tol, max_iter, parity=0, overlap=True, poll_every=4):
+    """Multishift CG of inverter_cgm.cpp:17-87 on FP64 slab fields.  shifts_ref: reference semantics (x_0 solves
+    shifts[0] - DD, x_j solves shifts[0] + shifts[j] - DD); stops shift k when Z_k^2 |r|^2 < tol.  Returns
+    (xs, iterations) with xs[r][k] the local solution of shift k on slab r.
+
+    Device-driven: the scalar recurrences run on a device state (kq_slab_cgm_*), each of the two reductions per
+    iteration is a device-side local sum and one in-place all-reduce over ranks (the reference's MPI_Allreduce,
+    spinor_field.cpp:207-215, 235-243), the shift vectors are updated in one fused pass, and the two dslash overlap
+    their halo exchange; everything is ordered on torch's current stream.  The host reads the state once every
+    poll_every iterations (steps after the stop are no-ops, so the iteration count is the reference's)."""
+    return _cgm(slabs, transport, bs, shifts_ref, tol, max_iter, parity, overlap, poll_every)
+
+
+def cgm_mixed(slabs, transport, bs, shifts_ref, rel_residual, max_iter, parity=0, sloppy=L.KUQCD_HALF, overlap=True,
+              poll_every=4, eps32=3e-7, eps16=1e-3, relax_frac=0.3, stop_frac=0.7, max_refine=4):
+    """The single-GPU mixed solver's schedule over slabs: a relaxed-precision multishift CG (operator on FP64 links
+    while |r| >= rho32 |b|, then FP32, then -- sloppy = HALF -- HALF below rho16 |b|, with rho = relax_frac *
+    rel_residual / eps; all vectors and scalars FP64; the precision is chosen at every poll), stopped at stop_frac *
+    rel_residual, then every shift's FP64 true residual |b - (sigma_k - DD) x_k| / |b| checked and, above
+    rel_residual, refined by FP64 slab CG on the residual.  Returns (xs, info): info["iterations"],
+    info["refine_iterations"], info["true_residuals"] (per shift) and info["iterations_by_precision"]."""
+    D = L.KUQCD_DOUBLE
+    bb = _global_dot(slabs, transport, bs, bs)
+    rho32 = relax_frac * rel_residual / eps32
+    rho16 = relax_frac * rel_residual / eps16 if sloppy == L.KUQCD_HALF else 0.0
+
+    def choose(rr):
+        rel2 = rr / bb
+        if rho16 > 0.0 and rel2 < rho16 * rho16:
+            return L.KUQCD_HALF
+        return L.KUQCD_SINGLE if rel2 < rho32 * rho32 else D
+
+    log = {}
+    xs, it = _cgm(slabs, transport, bs, shifts_ref, (stop_frac * rel_residual) ** 2 * bb, max_iter, parity, overlap,
+                  poll_every, choose=choose, log=log)
+    sig = [shifts_ref[0]] + [shifts_ref[0] + s for s in shifts_ref[1:]]
+    tmp = [s.field() for s in slabs]
+    res = [s.field() for s in slabs]
+    refine_it, true_res = 0, []
+    for k, sk in enumerate(sig):
+        xk = [xr[k] for xr in xs]
+        for attempt in range(max_refine + 1):
+            # res = b - (sigma_k - D D) x_k in FP64
+            dslash(slabs, transport, D, xk, tmp, 1 - parity, overlap=overlap)
+            dslash(slabs, transport, D, tmp, res, parity, pvecs=xk, sigma=sk, overlap=overlap)
+            for r, s in enumerate(slabs):
+                s.axpby(1.0, bs[r], -1.0, res[r])
+            rel = float(np.sqrt(max(_global_dot(slabs, transport, res, res), 0.0) / bb))
+            if rel <= rel_residual or attempt == max_refine:
+                break
+            es, its = _cgm(slabs, transport, res, [sk], (0.5 * rel_residual) ** 2 * bb, max_iter, parity, overlap,
+                           poll_every)
+            refine_it += its
+            for r, s in enumerate(slabs):
+                s.axpby(1.0, es[r][0], 1.0, xk[r])
+        true_res.append(rel)
+    torch.cuda.synchronize()
+    names = {L.KUQCD_DOUBLE: "double", L.KUQCD_SINGLE: "single", L.KUQCD_HALF: "half"}
+    return xs, {"iterations": it, "refine_iterations": refine_it, "true_residuals": true_res,
+                "iterations_by_precision": {names[p]: n for p, n in log.items()}}

@@ -99,6 +99,11 @@ def test_slab_multishift_cg_solves_global_system(cuda, R, poll_every):
     xs, it = SL.cgm(slabs, tr, bs, refsh, tol, 5000, poll_every=poll_every)
     xo, ito = O.cgm(GDIMS, fat, lng, 0, refsh, b, tol, 5000)
     assert abs(it - ito) <= 1, (it, ito)  # same recurrences; reductions summed in another order
+    # stream-ordered and deterministic: the same solve again gives the same count and the same bits
+    xs2, it2 = SL.cgm(slabs, tr, bs, refsh, tol, 5000, poll_every=poll_every)
+    assert it2 == it
+    for k in range(len(ab)):
+        assert torch.equal(torch.cat([xr[k] for xr in xs]), torch.cat([xr[k] for xr in xs2])), k
     for k in range(len(ab)):
         x = download(slabs, [xk[k] for xk in xs])
         assert np.abs(x - xo[k]).max() <= 1e-9 * np.abs(xo[k]).max()
@@ -146,3 +151,44 @@ def test_slab_cgm_zero_source_and_iteration_cap(cuda):
     b = O.make_source(GDIMS, 0, 9)
     xs, it = SL.cgm(slabs, tr, upload(slabs, b), [0.0025, 0.1], 1e-40, 7, poll_every=3)
     assert it == 7
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("R,sloppy", [(2, K.KUQCD_SINGLE), (2, K.KUQCD_HALF), (4, K.KUQCD_HALF)])
+def test_slab_mixed_cg_reaches_fp64_target(cuda, R, sloppy):
+    """The relaxed-precision multishift over slabs (FP64 -> FP32 -> HALF operator as |r| falls) plus the FP64 check /
+    refinement: every shift's true residual, recomputed by the oracle on the gathered solution, is at the target, and
+    the sloppy operators did run."""
+    slabs, tr, fat, lng = setup_slabs(R, 0.3, 15)
+    b = O.make_source(GDIMS, 0, 16)
+    m, sig = 0.05, np.logspace(-3, 0, 5)
+    ab = m * m + sig
+    refsh = [ab[0]] + list(sig[1:] - sig[0])
+    xs, info = SL.cgm_mixed(slabs, tr, upload(slabs, b), refsh, 1e-10, 5000, sloppy=sloppy)
+    assert len(info["true_residuals"]) == len(ab) and max(info["true_residuals"]) <= 1e-10, info
+    by = info["iterations_by_precision"]
+    assert by.get("double", 0) > 0 and by.get("single", 0) > 0, by
+    if sloppy == K.KUQCD_HALF:
+        assert by.get("half", 0) > 0, by
+    for k in range(len(ab)):
+        x = download(slabs, [xk[k] for xk in xs])
+        assert O.true_residual(GDIMS, fat, lng, 0, ab[k], b, x) <= 1.2e-10, k
+
+
+@pytest.mark.gpu
+def test_library_calls_follow_torch_stream(cuda):
+    """torch's default stream (handle 0) reaches the library as cudaStreamLegacy, never as NULL (which would mean the
+    context's own non-blocking stream, unordered with torch's work); a side stream reaches it as itself."""
+    from kuqcd_b200 import lib
+
+    assert lib._torch_stream(0).value == lib.CUDA_STREAM_LEGACY
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        assert lib._torch_stream(0).value == side.cuda_stream
+    # a buffer zero-filled by torch and then uploaded by the library holds the upload
+    slabs, tr, fat, lng = setup_slabs(1, 0.3, 17)
+    src = O.make_source(GDIMS, 1, 18)
+    for _ in range(3):
+        f = slabs[0].field()
+        slabs[0].ctx.upload(K.KUQCD_DOUBLE, SL.slab_of_spinor(src, GDIMS, 0, 1), f)
+        assert np.array_equal(download(slabs, [f]), src)
