@@ -41,7 +41,8 @@ struct SysDesc {
     LinkSet fat[3], lng[3];
     const void *b;
     void *x, *p0, *tmp, *ring, *pw;
-    size_t vb;
+    void *p0s;  // p0 in the operator precision of the FP32 / HALF phases (written by the p update), group-consecutive
+    size_t vb, vbs;
     double *partials;  // one per tile
     MsState *st;
 };
@@ -181,7 +182,8 @@ template <int BS, int M, int RP> struct Bounds {
 
 // K1: tmp_r = D p0_r and |tmp_r|^2 -> beta step with <p0, A p0> = sigma0 |p0|^2 + |tmp|^2 (|p0|^2 from the alpha
 // step's recurrence), for the members of each group whose operator precision is M (one launch per precision, so
-// that each launch is specialised; members in the other precisions are skipped).
+// that each launch is specialised; members in the other precisions are skipped).  In the FP32 / HALF phases p0 is
+// read from its copy in precision M.
 template <int BS, int M, int R, int P64>
 __global__ void __launch_bounds__(BS, Bounds<BS, M, Pass<M, R, P64>::v>::v) bk_dslash1_kernel(
     const int2 *__restrict__ items, int nitems, int spt)
@@ -207,8 +209,11 @@ __global__ void __launch_bounds__(BS, Bounds<BS, M, Pass<M, R, P64>::v>::v) bk_d
                 const unsigned u = (use >> base) & ((1u << RP) - 1u);
                 if (!u) continue;
                 T acc[RP][6];
-                dslash_site_mrhs_t<M, 0, T, RP>(d0.g, d0.pv, d0.fat[M], d0.lng[M],
-                                                static_cast<const char *>(d0.p0) + base * d0.vb, d0.vb, u,
+                // the FP32 / HALF phases gather p0 from its copy in their own precision (a third or half of the
+                // FP64 bytes through L1/L2 for each of the RP members)
+                const char *src = static_cast<const char *>(M == 0 ? d0.p0 : d0.p0s);
+                const size_t vbx = M == 0 ? d0.vb : d0.vbs;
+                dslash_site_mrhs_t<M, M, T, RP>(d0.g, d0.pv, d0.fat[M], d0.lng[M], src + base * vbx, vbx, u,
                                                 1 - d0.parity, i, acc);
 #pragma unroll
                 for (int r = 0; r < RP; ++r)
@@ -600,8 +605,8 @@ __global__ void __launch_bounds__(BS, Bounds<BS, M, 1>::v) bk_dslash2_staged_ker
     }
 }
 
-// K3: p0 = r^(i) + a0 p0; the next iteration's precision takes effect.  A system that stopped in K2 no longer
-// needs p0.
+// K3: p0 = r^(i) + a0 p0 (and its copy in the next iteration's precision when that is FP32 or HALF); the next
+// iteration's precision takes effect.  A system that stopped in K2 no longer needs p0.
 template <int BS>
 __global__ void __launch_bounds__(BS) bk_p0_kernel(const int2 *__restrict__ items, int nitems, int spt)
 {
@@ -613,6 +618,7 @@ __global__ void __launch_bounds__(BS) bk_p0_kernel(const int2 *__restrict__ item
         if (!st->active) continue;
         const char *r = static_cast<const char *>(d.ring) + (size_t)(st->iter % kWin) * d.vb;
         const double a0 = st->a[0];
+        const int nm = st->next_mode;  // the next iteration's operator precision (set by the alpha step)
         for (int sidx = 0; sidx < spt; ++sidx) {
             const int i = tile_site<BS>(w.y, spt, sidx);
             if (i >= d.g.vh) break;
@@ -622,6 +628,9 @@ __global__ void __launch_bounds__(BS) bk_p0_kernel(const int2 *__restrict__ item
 #pragma unroll
             for (int k = 0; k < 6; ++k) pv6[k] = rv[k] + a0 * pv6[k];
             st_spinor<0>(d.p0, d.pv, i, pv6);
+            // the copy the next K1 gathers from in the FP32 / HALF phases
+            if (nm == 1) st_spinor_as<1>(d.p0s, d.pv, i, pv6);
+            else if (nm == 2) st_spinor_as<2>(d.p0s, d.pv, i, pv6);
         }
         if (tile_ticket_last(&st->ticket[3], d.ntiles) && threadIdx.x == 0) {
             st->mode = st->next_mode;
@@ -921,10 +930,12 @@ cudaError_t batch_plan(kq_batch *b, int bs, int rhs, int spt, BatchPlan &plan, b
     for (size_t gi = 0; gi < plan.groups.size(); ++gi) {
         const GroupDesc &G = plan.groups[gi];
         const Geom &g = b->sys[G.mem[0]].ctx->g;
-        const size_t vb = spinor_bytes(g, P64);
+        const size_t vb = spinor_bytes(g, P64), vbs = spinor_bytes(g, P32);
         const int ntiles = (g.vh + tile - 1) / tile;
-        // the group's p0 and tmp fields are consecutive (the multi-RHS dslash addresses member r at base + r vb)
+        // the group's p0, sloppy p0 and tmp fields are consecutive (the multi-RHS dslash addresses member r at
+        // base + r vb); the sloppy copy holds FP32 or HALF, in FP32-sized slots
         char *p0 = static_cast<char *>(c.take(vb * G.n));
+        char *p0s = static_cast<char *>(c.take(vbs * G.n));
         char *tmp = static_cast<char *>(c.take(vb * G.n));
         for (int t = 0; t < ntiles; ++t) plan.grp_items.push_back(make_int2((int)gi, t));
         for (int r = 0; r < G.n; ++r) {
@@ -943,6 +954,8 @@ cudaError_t batch_plan(kq_batch *b, int bs, int rhs, int spt, BatchPlan &plan, b
                 d.lng[p] = ctx->gd.lng[p];
             }
             d.vb = vb;
+            d.vbs = vbs;
+            d.p0s = p0s ? p0s + r * vbs : nullptr;
             d.b = S.d_b;
             d.x = S.d_x;
             d.p0 = p0 ? p0 + r * vb : nullptr;
@@ -1000,7 +1013,7 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
     }
 
     // launch shape: tuned once per batch signature (sizes, shared gauge fields, shifts, schedule), cached on disk
-    std::string key = "batch5";
+    std::string key = "batch6";
     for (auto &S : b->sys) {
         int owner = 0;  // first system on the same context: systems sharing links share this number
         while (b->sys[owner].ctx != S.ctx) ++owner;
