@@ -154,10 +154,6 @@ KuQCDStatus kq_field_dot(kq_context *ctx, const void *d_x, const void *d_y, doub
 /* the local Re<x, y> into the device double *d_out, in stream order without a host round trip (an all-reduce over
  * ranks can then run on the device buffer) */
 KuQCDStatus kq_field_dot_device(kq_context *ctx, const void *d_x, const void *d_y, double *d_out, void *stream);
-/* the shift-vector updates of one CGM iteration (inverter_cgm.cpp:61-69) in one pass: for j < num_shift,
- * x_j -= B_j p_j, then p_j = Z_j r + a_j p_j; shift j's FP64 fields at d_p + j * stride and d_x + j * stride */
-KuQCDStatus kq_field_ms_update(kq_context *ctx, int num_shift, const double *B, const double *Z, const double *a,
-                               const void *d_r, void *d_p, void *d_x, size_t stride, void *stream);
 /* Device-driven multishift CG over slabs: the recurrences of CGM::Invert (inverter_cgm.cpp:17-87) on a state in
  * device memory, so that no step waits on the host.  Per iteration, in stream order on every rank:
  *   s = shifts_ref[0] p_0 - D D p_0 (two kq_slab_dslash with the halo exchange);

@@ -205,32 +205,6 @@ __global__ void field_sum_kernel(const double *__restrict__ partials, int n, dou
     if (threadIdx.x == 0) *out = s;
 }
 
-// the shift vectors of one multishift CG iteration (inverter_cgm.cpp:61-69): x_j -= B_j p_j, then
-// p_j = Z_j r + a_j p_j, for j < nshift; shift j's fields at base + j * stride
-struct MsCoef {
-    double B[kMaxShift], Z[kMaxShift], a[kMaxShift];
-};
-__global__ void field_ms_update_kernel(int vh, int pv, int nshift, MsCoef c, const void *__restrict__ r, char *p,
-                                       char *x, size_t stride)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= vh) return;
-    double rv[6];
-    ld_spinor<0>(r, pv, i, rv);
-    for (int j = 0; j < nshift; ++j) {
-        double pv6[6], xv[6];
-        ld_spinor<0>(p + j * stride, pv, i, pv6);
-        ld_spinor<0>(x + j * stride, pv, i, xv);
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            xv[k] -= c.B[j] * pv6[k];
-            pv6[k] = c.Z[j] * rv[k] + c.a[j] * pv6[k];
-        }
-        st_spinor<0>(x + j * stride, pv, i, xv);
-        st_spinor<0>(p + j * stride, pv, i, pv6);
-    }
-}
-
 // y = a x + b y on FP64 fields (pitch pv), and the block partials of <x, y>
 __global__ void field_axpby_kernel(int vh, int pv, double a, const void *__restrict__ x, double b, void *y)
 {
@@ -469,28 +443,6 @@ KQ_API KuQCDStatus kq_field_dot_device(kq_context *ctx, const void *d_x, const v
     double *partials = static_cast<double *>(ctx->work);
     field_dot_kernel<<<nb, 256, 0, s>>>(g.vh, pad_sites(g.vh), d_x, d_y, partials);
     field_sum_kernel<<<1, 256, 0, s>>>(partials, nb, d_out);
-    return status_of(cudaGetLastError());
-}
-
-KQ_API KuQCDStatus kq_field_ms_update(kq_context *ctx, int num_shift, const double *B, const double *Z,
-                                      const double *a, const void *d_r, void *d_p, void *d_x, size_t stride,
-                                      void *stream)
-{
-    if (!ctx || !B || !Z || !a || !d_r || !d_p || !d_x) return KUQCD_ERR_NULL_POINTER;
-    if (num_shift < 0 || num_shift > kMaxShift) return KUQCD_ERR_INVALID_PARAM;
-    if (num_shift == 0) return KUQCD_SUCCESS;
-    cudaSetDevice(ctx->device);
-    MsCoef c;
-    for (int j = 0; j < num_shift; ++j) {
-        c.B[j] = B[j];
-        c.Z[j] = Z[j];
-        c.a[j] = a[j];
-    }
-    const Geom &g = ctx->g;
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
-    field_ms_update_kernel<<<(g.vh + 255) / 256, 256, 0, s>>>(g.vh, pad_sites(g.vh), num_shift, c, d_r,
-                                                              static_cast<char *>(d_p), static_cast<char *>(d_x),
-                                                              stride);
     return status_of(cudaGetLastError());
 }
 

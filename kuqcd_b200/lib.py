@@ -67,7 +67,7 @@ EXPORTED_SYMBOLS = [
     "kq_mdagm_noalloc", "kq_dslash_full", "kq_mdagm_full", "kq_long_links_compressed", "kq_slab_set",
     "kq_slab_face_bytes", "kq_slab_pack_faces", "kq_slab_link_face_bytes", "kq_slab_pack_link_face", "kq_slab_set_link_ghosts",
     "kq_slab_dslash", "kq_slab_dslash_part", "kq_field_axpby", "kq_field_dot", "kq_field_dot_device",
-    "kq_field_ms_update", "kq_slab_cgm_state_bytes", "kq_slab_cgm_init", "kq_slab_cgm_step",
+    "kq_slab_cgm_state_bytes", "kq_slab_cgm_init", "kq_slab_cgm_step",
     "kq_slab_cgm_residual", "kq_slab_cgm_update", "kq_slab_cgm_poll", "kq_host_alloc", "kq_host_free", "kq_apply_host",
     "kq_vec_axpby", "kq_vec_dot",
     "kq_solve_multishift", "kq_solve_multishift_device", "kq_true_residuals", "kq_make_links_record",
@@ -139,7 +139,6 @@ def library() -> C.CDLL:
         "kq_field_dot": (i, [vp, vp, vp, C.POINTER(d)]),
         "kq_slab_dslash_part": (i, [vp, i, vp, vp, vp, vp, i, vp, d, i, vp]),
         "kq_field_dot_device": (i, [vp, vp, vp, vp, vp]),
-        "kq_field_ms_update": (i, [vp, i, C.POINTER(d), C.POINTER(d), C.POINTER(d), vp, vp, vp, sz, vp]),
         "kq_slab_cgm_state_bytes": (sz, []),
         "kq_slab_cgm_init": (i, [vp, vp, i, C.POINTER(d), d, i, vp]),
         "kq_slab_cgm_step": (i, [vp, vp, i, vp]),

@@ -76,10 +76,6 @@ class LocalTransport:
         tot = np.sum(np.asarray(values, dtype=np.float64), axis=0)
         return [tot.copy() for _ in values]
 
-    def allreduce_device(self, tensors):
-        """Sum of the ranks' device tensors, returned on the host (one synchronisation)."""
-        return torch.stack([t for t in tensors]).sum(0).cpu().numpy()
-
     def allreduce_inplace(self, tensors):
         """Every rank's device tensor becomes the sum over ranks, in stream order (no host synchronisation)."""
         tot = torch.stack([t.to(tensors[0].device) for t in tensors]).sum(0)
@@ -138,15 +134,6 @@ class TorchTransport:
         t = torch.tensor(np.asarray(v, dtype=np.float64), device=dev)
         self.dist.all_reduce(t, group=self.group)
         return [t.cpu().numpy()]
-
-    def allreduce_device(self, tensors):
-        """One all-reduce of this rank's device tensor (NCCL on the device; gloo through the host), returned on the
-        host."""
-        (t,) = tensors
-        if self.dist.get_backend(self.group) != "nccl":
-            t = t.cpu()
-        self.dist.all_reduce(t, group=self.group)
-        return t.cpu().numpy()
 
     def allreduce_inplace(self, tensors):
         """This rank's tensor becomes the sum over ranks: NCCL on the device in stream order (no host
@@ -218,15 +205,6 @@ class Slab:
         """local <x, y> into out (a one-element float64 device tensor), without a host round trip"""
         self.ctx._chk(L.library().kq_field_dot_device(self.ctx._h, _p(x), _p(y), _p(out), self.stream()),
                       "kq_field_dot_device")
-
-    def ms_update(self, B, Z, a, r, p_block, x_block, n):
-        """x_j -= B_j p_j ; p_j = Z_j r + a_j p_j for j < n (shift j's fields at block + j * field bytes)"""
-        vb = self.ctx.spinor_bytes(L.KUQCD_DOUBLE)
-        arr = [np.ascontiguousarray(v[:max(n, 1)], dtype=np.float64) for v in (B, Z, a)]
-        ptr = [v.ctypes.data_as(C.POINTER(C.c_double)) for v in arr]
-        self.ctx._chk(L.library().kq_field_ms_update(self.ctx._h, n, *ptr, _p(r), _p(p_block), _p(x_block), vb,
-                                                     self.stream()),
-                      "kq_field_ms_update")
 
     def axpby(self, a, x, b, y):
         self.ctx._chk(L.library().kq_field_axpby(self.ctx._h, float(a), _p(x), float(b), _p(y), self.stream()),
