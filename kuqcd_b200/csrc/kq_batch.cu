@@ -29,6 +29,7 @@
 
 #include "kq_context.h"
 #include "kq_dslash_core.cuh"
+#include "kq_dslash_half2.cuh"
 #include "kq_ms_device.cuh"
 #include "kq_msrelax.h"
 #include "kq_tune.h"
@@ -106,6 +107,96 @@ __device__ __forceinline__ unsigned group_mask(const GroupDesc &G)
             if (st->active && st->mode == M) use |= 1u << r;
         }
     return use;
+}
+
+// ------------------------------------------------------------------ grouped dslash of one site, FP32 arithmetic
+// With several members the FP32 / HALF grouped kernels are instruction-bound: the link is loaded once, but every
+// member needs its own mat-vecs.  Members 2q and 2q + 1 therefore share f32x2 registers (low half member 2q), every
+// link element is duplicated into both halves once per link (negated for the backward hops, so that one accumulator
+// takes all sixteen terms), and each packed FMA serves two members: 36 f32x2 FMAs per pair and link instead of 72.
+// Same terms in the same order as dslash_site_mrhs_t; a member outside `use` enters as zeros.
+template <int SP>
+__device__ __forceinline__ void ld_member_pair(const char *src0, size_t stride, int r0, unsigned use, int pv, int n,
+                                               h2::f2 v[6])
+{
+    float a[6], b[6];
+    if (use & (1u << r0)) ld_spinor_as<SP>(src0 + (size_t)r0 * stride, pv, n, a);
+    else
+#pragma unroll
+        for (int k = 0; k < 6; ++k) a[k] = 0.f;
+    if (use & (2u << r0)) ld_spinor_as<SP>(src0 + (size_t)(r0 + 1) * stride, pv, n, b);
+    else
+#pragma unroll
+        for (int k = 0; k < 6; ++k) b[k] = 0.f;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) v[k] = h2::pack(a[k], b[k]);
+}
+
+template <int LP, int SP, int RP>
+__device__ __forceinline__ void dslash_site_mrhs_pair(const Geom &g, int pv, const LinkSet &fat, const LinkSet &lng,
+                                                      const char *src0, size_t stride, unsigned use, int p, int i,
+                                                      float acc[RP][6])
+{
+    using namespace h2;
+    static_assert(RP % 2 == 0, "members come in pairs");
+    constexpr int NP = RP / 2;
+    const SiteCoord c = site_coord(g, i, p);
+    const void *fat_p = p ? fat.par[1] : fat.par[0], *fat_q = p ? fat.par[0] : fat.par[1];
+    const void *lng_p = p ? lng.par[1] : lng.par[0], *lng_q = p ? lng.par[0] : lng.par[1];
+    const float rl = fold_scale_long<LP, float>(fat, lng);
+    const f2 rl2 = pack(rl, rl), m1 = pack(-1.f, -1.f);
+    f2 a2[NP][6];
+#pragma unroll
+    for (int q = 0; q < NP; ++q)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) a2[q][k] = pack(0.f, 0.f);
+#pragma unroll
+    for (int dir = 0; dir < 4; ++dir) {
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {  // fat forward, long forward, fat backward, long backward
+            const bool bwd = h >= 2, isl = (h & 1) != 0;
+            const int n = nbr_index(g, c, i, dir, h == 0 ? 1 : h == 1 ? 3 : h == 2 ? -1 : -3);
+            const LinkSet &L = isl ? lng : fat;
+            float u[18];
+            ld_link_fold<LP>(h == 0 ? fat_p : h == 1 ? lng_p : h == 2 ? fat_q : lng_q, pv, dir, bwd ? n : i, L, u);
+            f2 uu[18];
+#pragma unroll
+            for (int k = 0; k < 18; ++k) uu[k] = bwd ? pack(-u[k], -u[k]) : pack(u[k], u[k]);
+#pragma unroll
+            for (int q = 0; q < NP; ++q) {
+                if (!(use & (3u << (2 * q)))) continue;
+                f2 v[6], w[3];
+                ld_member_pair<SP>(src0, stride, 2 * q, use, pv, n, v);
+                if (LP == 2 && isl)
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) v[k] = mul2(v[k], rl2);
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc) w[cc] = mul2(v[2 * cc + (bwd ? 0 : 1)], m1);
+                if (bwd) mdv_add2(uu, v, w, a2[q]);  // + (-U)^dag v
+                else mv_add2(uu, v, w, a2[q]);
+            }
+        }
+    }
+    const float sf = LP == 2 ? fat.scale * (1.0f / 32767.0f) : 1.0f;
+#pragma unroll
+    for (int q = 0; q < NP; ++q)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            float lo, hi;
+            unpack(a2[q][k], lo, hi);
+            acc[2 * q][k] = LP == 2 ? lo * sf : lo;
+            acc[2 * q + 1][k] = LP == 2 ? hi * sf : hi;
+        }
+}
+
+// the grouped dslash of one site: FP32 arithmetic with an even member count in the packed member-pair form
+template <int M, int SP, typename T, int RP>
+__device__ __forceinline__ void grouped_site(const Geom &g, int pv, const LinkSet &fat, const LinkSet &lng,
+                                             const char *src0, size_t stride, unsigned use, int p, int i,
+                                             T acc[RP][6])
+{
+    if constexpr (M != 0 && RP % 2 == 0) dslash_site_mrhs_pair<M, SP, RP>(g, pv, fat, lng, src0, stride, use, p, i, acc);
+    else dslash_site_mrhs_t<M, SP, T, RP>(g, pv, fat, lng, src0, stride, use, p, i, acc);
 }
 
 // Members per pass over a tile: every pass loads the links once for its members.  FP64 accumulators take twice the
@@ -213,7 +304,7 @@ __global__ void __launch_bounds__(BS, Bounds<BS, M, Pass<M, R, P64>::v>::v) bk_d
                 // FP64 bytes through L1/L2 for each of the RP members)
                 const char *src = static_cast<const char *>(M == 0 ? d0.p0 : d0.p0s);
                 const size_t vbx = M == 0 ? d0.vb : d0.vbs;
-                dslash_site_mrhs_t<M, M, T, RP>(d0.g, d0.pv, d0.fat[M], d0.lng[M], src + base * vbx, vbx, u,
+                grouped_site<M, M, T, RP>(d0.g, d0.pv, d0.fat[M], d0.lng[M], src + base * vbx, vbx, u,
                                                 1 - d0.parity, i, acc);
 #pragma unroll
                 for (int r = 0; r < RP; ++r)
@@ -271,7 +362,7 @@ __global__ void __launch_bounds__(BS, Bounds<BS, M, Pass<M, R, P64>::v>::v) bk_d
                 const unsigned u = (use >> base) & ((1u << RP) - 1u);
                 if (!u) continue;
                 T acc[RP][6];
-                dslash_site_mrhs_t<M, M, T, RP>(d0.g, d0.pv, d0.fat[M], d0.lng[M],
+                grouped_site<M, M, T, RP>(d0.g, d0.pv, d0.fat[M], d0.lng[M],
                                                 static_cast<const char *>(d0.tmp) + base * d0.vb, d0.vb, u,
                                                 d0.parity, i, acc);
 #pragma unroll
