@@ -63,15 +63,17 @@ __global__ void __launch_bounds__(256) dslash_full_kernel(Geom g, int pv, LinkSe
     st_spinor<SP>(dst + p * half, pv, i, acc);
 }
 
-// HALF kernel: 0 one site per thread, 4 / 5 two sites per thread in packed FP32 with 4 / 5 resident 128-thread
-// CTAs per SM (KUQCD_HALF_DSLASH = site | pair4 | pair5; default pair5)
+// HALF kernel: 0 one site per thread, 4 .. 7 two sites per thread in packed FP32 with 4 .. 7 resident 128-thread
+// CTAs per SM (KUQCD_HALF_DSLASH = site | pair4 | pair5 | pair6 | pair7).  Default pair7: the kernel is latency-
+// bound, and 28 warps per SM at 72 registers (40 B of spills) beat 20 at 96 (48^3x96: 536 against 577 us).
 static int half_kernel()
 {
     static const int k = [] {
         const char *e = getenv("KUQCD_HALF_DSLASH");
-        if (!e) return 5;
+        if (!e) return 7;
         if (e[0] == 's') return 0;
-        return strcmp(e, "pair4") == 0 ? 4 : 5;
+        if (strncmp(e, "pair", 4) == 0 && e[4] >= '4' && e[4] <= '7' && e[5] == 0) return e[4] - '0';
+        return 7;
     }();
     return k;
 }
@@ -99,10 +101,12 @@ cudaError_t launch_dslash2(const Geom &g, const GaugeDev &gd, int lp, int sp, co
         // HALF: two sites per thread in packed FP32 (kq_dslash_half2.cuh)
         constexpr int kBS2 = 128;
         const int nb2 = (g.vh + 2 * kBS2 - 1) / (2 * kBS2);
-        if (half_kernel() == 4)
-            dslash_half2_kernel<kBS2, 4><<<nb2, kBS2, 0, s>>>(g, pv, gd.fat[lp], gd.lng[lp], src, dst, dst_parity);
-        else
-            dslash_half2_kernel<kBS2, 5><<<nb2, kBS2, 0, s>>>(g, pv, gd.fat[lp], gd.lng[lp], src, dst, dst_parity);
+        switch (half_kernel()) {
+            case 4: dslash_half2_kernel<kBS2, 4><<<nb2, kBS2, 0, s>>>(g, pv, gd.fat[lp], gd.lng[lp], src, dst, dst_parity); break;
+            case 6: dslash_half2_kernel<kBS2, 6><<<nb2, kBS2, 0, s>>>(g, pv, gd.fat[lp], gd.lng[lp], src, dst, dst_parity); break;
+            case 7: dslash_half2_kernel<kBS2, 7><<<nb2, kBS2, 0, s>>>(g, pv, gd.fat[lp], gd.lng[lp], src, dst, dst_parity); break;
+            default: dslash_half2_kernel<kBS2, 5><<<nb2, kBS2, 0, s>>>(g, pv, gd.fat[lp], gd.lng[lp], src, dst, dst_parity); break;
+        }
         return cudaGetLastError();
     }
     const int bs = block > 0 ? block : 256;
