@@ -255,14 +255,14 @@ def run_lattice(cfg, args, rank, world, local, steps, warmup, plain_steps, e2e_s
                     launches=launches, true_res=max(true_res), sloppy_res=info.sloppy_residual, steps=nsteps,
                     clocks=clk.summary() if clk else None)
 
-    main_run = timed(args.solver, steps, warmup, clocks)
-    plain = timed("fp64", plain_steps, 1, False) if args.solver != "fp64" else None
-    plain_w = timed("fp64w", plain_steps, 1, False) if windowed and args.solver not in ("fp64", "fp64w") else None
-
-    # ---------------- dslash in three precisions: CUDA events on the (non-default) stream the kernels run on
+    # ---------------- dslash in three precisions: CUDA events on the (non-default) stream the kernels run on.  Timed
+    # alone, before the solves (compared with the burst copy peak), with the SM clocks sampled meanwhile.
     dsl = {}
     stream = torch.cuda.Stream()
     peak, _ = measured_peak()
+    dclk = ClockSampler(local) if clocks else None
+    if dclk:
+        dclk.__enter__()
     for name, prec in [("fp64", K.KUQCD_DOUBLE), ("fp32", K.KUQCD_SINGLE), ("half", K.KUQCD_HALF)]:
         nbp = ctx.spinor_bytes(prec)
         a = torch.zeros(nbp, dtype=torch.uint8, device="cuda")
@@ -285,6 +285,14 @@ def run_lattice(cfg, args, rank, world, local, steps, warmup, plain_steps, e2e_s
                      "bytes_per_site": moved, "compulsory_bytes_per_site": DSLASH_BYTES[prec],
                      "compulsory_gbs": DSLASH_BYTES[prec] * Vh / t / 1e9, "long_links_compressed": bool(rc == 1)}
         del a, o
+    if dclk:
+        dclk.__exit__(None, None, None)
+        dsl["clocks"] = dclk.summary()
+
+    main_run = timed(args.solver, steps, warmup, clocks)
+    plain = timed("fp64", plain_steps, 1, False) if args.solver != "fp64" else None
+    plain_w = timed("fp64w", plain_steps, 1, False) if windowed and args.solver not in ("fp64", "fp64w") else None
+
     long_recon = ctx.long_links_compressed(K.KUQCD_DOUBLE)
     ctx.close()  # free its links and workspace before the API path loads its own copy
     del d_b, d_x
@@ -430,10 +438,10 @@ def run_ours(args):
             if small["plain_w"] is not None:
                 result["lattice_32"]["plain_fp64"]["windowed"] = plain_info(small["plain_w"], sm["ms"], world)
         if small is not None and world == 1:
-            # the batched workloads (24 systems on three lattices), one timed step each after a warm-up step that
-            # includes the shape tuning: their own lines come from --config batch / batch-rhs
+            # the batched workloads (24 systems on three lattices): two warm-up steps (the first tunes the launch
+            # shape), the median of three timed steps; their own lines come from --config batch / batch-rhs
             bargs = argparse.Namespace(**vars(args))
-            bargs.steps, bargs.warmup = 1, 1
+            bargs.steps, bargs.warmup = 3, 2
             for name, shared in (("batch", False), ("batch_rhs", True)):
                 b = run_batch(bargs, shared=shared, emit=False)
                 result[name] = {k: b[k] for k in ("value", "unit", "ms_per_step", "steps", "warmup", "config",
