@@ -364,6 +364,22 @@ def cgm(slabs, transport, bs, shifts_ref, tol, max_iter, parity=0, overlap=True,
     return _cgm(slabs, transport, bs, shifts_ref, tol, max_iter, parity, overlap, poll_every)
 
 
+def relaxed_thresholds(rel_residual, sloppy=L.KUQCD_HALF, eps32=3e-7, eps16=1e-3, relax_frac=0.3):
+    """(rho32, rho16) of the relaxed-precision schedule: the operator may run on FP32 links below |r| = rho32 |b| and
+    on HALF links below rho16 |b| (0: no HALF phase), rho = relax_frac * target / eps (the single-GPU mixed
+    solver's rule: a matvec error eps |A| |p| made at |r| = rho |b| perturbs the final residual by about eps rho)."""
+    rho32 = relax_frac * rel_residual / eps32
+    rho16 = relax_frac * rel_residual / eps16 if sloppy == L.KUQCD_HALF else 0.0
+    return rho32, rho16
+
+
+def relaxed_precision(rel2, rho32, rho16):
+    """The operator precision for a squared relative residual |r|^2 / |b|^2."""
+    if rho16 > 0.0 and rel2 < rho16 * rho16:
+        return L.KUQCD_HALF
+    return L.KUQCD_SINGLE if rel2 < rho32 * rho32 else L.KUQCD_DOUBLE
+
+
 def cgm_mixed(slabs, transport, bs, shifts_ref, rel_residual, max_iter, parity=0, sloppy=L.KUQCD_HALF, overlap=True,
               poll_every=4, eps32=3e-7, eps16=1e-3, relax_frac=0.3, stop_frac=0.7, max_refine=4):
     """The single-GPU mixed solver's schedule over slabs: a relaxed-precision multishift CG (operator on FP64 links
@@ -374,14 +390,10 @@ def cgm_mixed(slabs, transport, bs, shifts_ref, rel_residual, max_iter, parity=0
     info["refine_iterations"], info["true_residuals"] (per shift) and info["iterations_by_precision"]."""
     D = L.KUQCD_DOUBLE
     bb = _global_dot(slabs, transport, bs, bs)
-    rho32 = relax_frac * rel_residual / eps32
-    rho16 = relax_frac * rel_residual / eps16 if sloppy == L.KUQCD_HALF else 0.0
+    rho32, rho16 = relaxed_thresholds(rel_residual, sloppy, eps32, eps16, relax_frac)
 
     def choose(rr):
-        rel2 = rr / bb
-        if rho16 > 0.0 and rel2 < rho16 * rho16:
-            return L.KUQCD_HALF
-        return L.KUQCD_SINGLE if rel2 < rho32 * rho32 else D
+        return relaxed_precision(rr / bb, rho32, rho16)
 
     log = {}
     xs, it = _cgm(slabs, transport, bs, shifts_ref, (stop_frac * rel_residual) ** 2 * bb, max_iter, parity, overlap,

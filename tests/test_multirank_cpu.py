@@ -132,3 +132,16 @@ def test_slab_exchange_with_a_dead_peer_fails_with_an_error(tmp_path):
     mp.spawn(_dead_peer_worker, args=(2, free_port(), str(tmp_path)), nprocs=2, join=True)
     outcome = (tmp_path / "r0.txt").read_text()
     assert outcome.startswith("error"), outcome
+
+
+def test_slab_relaxed_precision_schedule():
+    """The slab mixed solver's precision schedule: FP64 until |r| < rho32 |b|, FP32 until rho16 |b|, then HALF, with
+    the single-GPU solver's thresholds (target 1e-10: rho32 = 1e-4, rho16 = 3e-8); no HALF phase for sloppy FP32."""
+    import kuqcd_b200 as K
+
+    r32, r16 = SL.relaxed_thresholds(1e-10)
+    assert np.isclose(r32, 1e-4) and np.isclose(r16, 3e-8)
+    assert SL.relaxed_thresholds(1e-10, sloppy=K.KUQCD_SINGLE)[1] == 0.0
+    pick = [SL.relaxed_precision(rel ** 2, r32, r16) for rel in (1.0, 2e-4, 9e-5, 1e-6, 4e-8, 2e-8, 1e-10)]
+    assert pick == [K.KUQCD_DOUBLE] * 2 + [K.KUQCD_SINGLE] * 3 + [K.KUQCD_HALF] * 2
+    assert SL.relaxed_precision(1e-20, r32, 0.0) == K.KUQCD_SINGLE
