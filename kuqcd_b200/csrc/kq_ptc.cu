@@ -242,8 +242,8 @@ __global__ void __launch_bounds__(kThr) ptc_forward_kernel(Geom g, int pv, LinkS
 // latency.  Chunk j's MMAs commit to mbarrier (j & 1); before chunk j + 2 overwrites that buffer every thread waits
 // for the commit's phase (j >> 1) & 1 (bounded, as in the whole-tile kernel).
 constexpr uint32_t kChunkColBytes = kTile * 16 * 2;  // one colour's [128 x 16] BF16 chunk
-template <int COUT>
-__global__ void __launch_bounds__(kThr, 4) ptc_forward8_kernel(Geom g, int pv, LinkSet fat, const float2 *__restrict__ in,
+template <int COUT, int MINB>
+__global__ void __launch_bounds__(kThr, MINB) ptc_forward8_kernel(Geom g, int pv, LinkSet fat, const float2 *__restrict__ in,
                                                             float2 *__restrict__ out, const __nv_bfloat16 *__restrict__ Bt,
                                                             int swap_paths, int *fault)
 {
@@ -628,18 +628,44 @@ cudaError_t ptc_raise_fault_for_test()
     return cudaMemcpy(f, &one, sizeof(int), cudaMemcpyHostToDevice);
 }
 
-template <int COUT>
-static cudaError_t run_forward8(const Geom &g, const LinkSet &fat, const float2 *in, float2 *out,
-                                const __nv_bfloat16 *Bt, bool swap, cudaStream_t s)
+// Resident CTAs per SM the 8-channel kernel is compiled for (KUQCD_PTC_CTAS = 4 .. 7; 64 TMEM columns and 29 KB of
+// shared memory each, so 7 fit the SM's 512 columns and 228 KB).  The gather is latency-bound: six CTAs at 80
+// registers (8 B spilled) apply M in 1.50 ms at 32^4 against 1.79 ms for four at 128.
+static int ptc_ctas()
+{
+    static const int k = [] {
+        const char *e = getenv("KUQCD_PTC_CTAS");
+        const int v = e ? atoi(e) : 6;
+        return v >= 4 && v <= 7 ? v : 6;
+    }();
+    return k;
+}
+
+template <int COUT, int MINB>
+static cudaError_t run_forward8_b(const Geom &g, const LinkSet &fat, const float2 *in, float2 *out,
+                                  const __nv_bfloat16 *Bt, bool swap, cudaStream_t s)
 {
     const int pv = pad_sites(g.vh);
     const int tiles = 2 * ((g.vh + kTile - 1) / kTile);
     const size_t sm = (size_t)2 * 3 * kChunkColBytes + (size_t)kNT * kpad_of(8) * 2 + 32;
-    KQ_CUDA_TRY(cudaFuncSetAttribute(ptc_forward8_kernel<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    KQ_CUDA_TRY(cudaFuncSetAttribute(ptc_forward8_kernel<COUT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sm));
     int *fault = fault_flag();
     if (!fault) return cudaErrorInvalidDevicePointer;
-    ptc_forward8_kernel<COUT><<<tiles, kThr, sm, s>>>(g, pv, fat, in, out, Bt, swap ? 1 : 0, fault);
+    ptc_forward8_kernel<COUT, MINB><<<tiles, kThr, sm, s>>>(g, pv, fat, in, out, Bt, swap ? 1 : 0, fault);
     return cudaGetLastError();
+}
+
+template <int COUT>
+static cudaError_t run_forward8(const Geom &g, const LinkSet &fat, const float2 *in, float2 *out,
+                                const __nv_bfloat16 *Bt, bool swap, cudaStream_t s)
+{
+    switch (ptc_ctas()) {
+        case 4: return run_forward8_b<COUT, 4>(g, fat, in, out, Bt, swap, s);
+        case 5: return run_forward8_b<COUT, 5>(g, fat, in, out, Bt, swap, s);
+        case 7: return run_forward8_b<COUT, 7>(g, fat, in, out, Bt, swap, s);
+        default: return run_forward8_b<COUT, 6>(g, fat, in, out, Bt, swap, s);
+    }
 }
 
 template <int CIN, int COUT>
