@@ -266,9 +266,11 @@ __global__ void __launch_bounds__(BS) bk_init_kernel(const int2 *__restrict__ it
 
 // Launch bounds of the dslash kernels: one group member (R = 1) keeps the single-system shapes (FP32: three
 // 256-thread CTAs per SM; FP64 and HALF up to 128 registers, at the 85-register cap the long-link row rebuild and
-// the HALF decode spill); several members need room for their accumulators (FP64: one 256-thread CTA per SM).
+// the HALF decode spill); several members need room for their accumulators (FP64: one 256-thread CTA per SM).  The
+// FP32 / HALF kernels of 2 or 4 members (dslash_site_mrhs_pair) are latency-bound and take three
+// 256-thread CTAs per SM at 80 registers (at most 32 B spilled); 8 members keep two (they would spill ~1 KB).
 template <int BS, int M, int RP> struct Bounds {
-    static constexpr int v = RP == 1 ? (M == 1 ? 768 : 512) / BS : (M == 0 ? 256 : 512) / BS;
+    static constexpr int v = RP == 1 ? (M == 1 ? 768 : 512) / BS : (M == 0 ? 256 : RP <= 4 ? 768 : 512) / BS;
 };
 
 // K1: tmp_r = D p0_r and |tmp_r|^2 -> beta step with <p0, A p0> = sigma0 |p0|^2 + |tmp|^2 (|p0|^2 from the alpha
@@ -1104,7 +1106,7 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
     }
 
     // launch shape: tuned once per batch signature (sizes, shared gauge fields, shifts, schedule), cached on disk
-    std::string key = "batch6";
+    std::string key = "batch7";
     for (auto &S : b->sys) {
         int owner = 0;  // first system on the same context: systems sharing links share this number
         while (b->sys[owner].ctx != S.ctx) ++owner;
@@ -1217,7 +1219,8 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
         // CTAs per SM on two windows, with every shared gauge field serving as many right-hand sides as it can;
         // per group width, the FP64 pass mode on two windows (the solve's first windows run on FP64 links); the
         // group widths against each other on complete solves (the width also sets the sloppy kernels' register
-        // use, which the first windows do not see); then the sites per thread.
+        // use, which the first windows do not see); CTAs per SM again for that width, on complete solves; then the
+        // sites per thread.
         auto timed = [&](const BatchTune &t, int chunks, float *ms) -> cudaError_t {
             long long l = 0;
             int ch = 0, ng = 0;
@@ -1274,6 +1277,23 @@ static KuQCDStatus solve_batched(kq_batch *b, kq_batch_info *out)
                 if (ms < best) {
                     best = ms;
                     tune = wbest;
+                }
+            }
+        }
+        if (rmax > 1) {
+            // CTAs per SM of the persistent grid again, for the chosen width (its kernels' residency differs from
+            // the widest group's, on which the first sweep ran), on complete solves
+            const BatchTune w = tune;
+            for (int cps : {4, 8, 16}) {
+                if (cps == w.ctas_per_sm || (w.bs == 256 && cps > 8)) continue;
+                BatchTune c = w;
+                c.ctas_per_sm = cps;
+                float ms;
+                const cudaError_t e = timed(c, 0, &ms);
+                if (e != cudaSuccess) return status_of(e);
+                if (ms < best) {
+                    best = ms;
+                    tune = c;
                 }
             }
         }
