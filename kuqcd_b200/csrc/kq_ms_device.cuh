@@ -142,7 +142,25 @@ __device__ __forceinline__ void ms_step_alpha(MsState *st, double lambda2)
 // Windowed shift update of one site, one colour component at a time (keeps W ring values in registers, not 6 W):
 //   p_k <- c_k p_k + sum_l d_kl r_l ,  x_k <- x_k + e_k p_k + sum_l f_kl r_l   for k < kmax.
 // Window position l (0-based) holds r^(i0+l+1) in ring slot (l+1) % W; positions >= n are unused (zero weight).
-// FP64 spinor fields are three double2 planes of pv sites (kq_prec.cuh).
+// FP64 spinor fields are three double2 planes of pv sites (kq_prec.cuh).  KU shifts at a time: their p and x are
+// loaded before any of them is stored (the stores could alias later loads for the compiler), so KU x 2 loads per
+// thread are in flight instead of 2.
+__device__ __forceinline__ void window_update_one(const double2 p, const double2 x, const double2 *rl, double c,
+                                                  double e, const double *d, const double *f, double2 &pn,
+                                                  double2 &xn)
+{
+    pn = make_double2(c * p.x, c * p.y);
+    xn = make_double2(x.x + e * p.x, x.y + e * p.y);
+#pragma unroll
+    for (int l = 0; l < kWin; ++l) {
+        pn.x += d[l] * rl[l].x;
+        pn.y += d[l] * rl[l].y;
+        xn.x += f[l] * rl[l].x;
+        xn.y += f[l] * rl[l].y;
+    }
+}
+
+template <int KU = 1>
 __device__ __forceinline__ void window_update_site(const char *ring, size_t vb, int pv, int i, int n, int kmax,
                                                    const double *sc, const double *se, const double (*sd)[kWin],
                                                    const double (*sf)[kWin], char *pw0, char *x0)
@@ -155,19 +173,29 @@ __device__ __forceinline__ void window_update_site(const char *ring, size_t vb, 
         for (int l = 0; l < kWin; ++l)
             rl[l] = l < n ? __ldg(reinterpret_cast<const double2 *>(ring + (size_t)((l + 1) % kWin) * vb) + off)
                           : make_double2(0.0, 0.0);
-        for (int k = 0; k < kmax; ++k) {
+        int k = 0;
+#pragma unroll 1
+        for (; k + KU <= kmax; k += KU) {
+            double2 p[KU], x[KU];
+#pragma unroll
+            for (int u = 0; u < KU; ++u) {
+                p[u] = reinterpret_cast<const double2 *>(pw0 + (k + u) * vb)[off];
+                x[u] = reinterpret_cast<const double2 *>(x0 + (k + u) * vb)[off];
+            }
+#pragma unroll
+            for (int u = 0; u < KU; ++u) {
+                double2 pn, xn;
+                window_update_one(p[u], x[u], rl, sc[k + u], se[k + u], sd[k + u], sf[k + u], pn, xn);
+                reinterpret_cast<double2 *>(pw0 + (k + u) * vb)[off] = pn;
+                reinterpret_cast<double2 *>(x0 + (k + u) * vb)[off] = xn;
+            }
+        }
+#pragma unroll 1
+        for (; k < kmax; ++k) {
             double2 *pp = reinterpret_cast<double2 *>(pw0 + k * vb) + off;
             double2 *xp = reinterpret_cast<double2 *>(x0 + k * vb) + off;
-            const double2 p = *pp, x = *xp;
-            double2 pn = make_double2(sc[k] * p.x, sc[k] * p.y);
-            double2 xn = make_double2(x.x + se[k] * p.x, x.y + se[k] * p.y);
-#pragma unroll
-            for (int l = 0; l < kWin; ++l) {
-                pn.x += sd[k][l] * rl[l].x;
-                pn.y += sd[k][l] * rl[l].y;
-                xn.x += sf[k][l] * rl[l].x;
-                xn.y += sf[k][l] * rl[l].y;
-            }
+            double2 pn, xn;
+            window_update_one(*pp, *xp, rl, sc[k], se[k], sd[k], sf[k], pn, xn);
             *pp = pn;
             *xp = xn;
         }

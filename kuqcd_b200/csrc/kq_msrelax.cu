@@ -164,7 +164,8 @@ __global__ void __launch_bounds__(kBSm) ms_p0_kernel(int vh, int pv, const char 
 }
 
 // K4: windowed shift update p_k <- c_k p_k + sum_l d_kl r_l ; x_k <- x_k + e_k p_k + sum_l f_kl r_l
-__global__ void __launch_bounds__(kBSm) ms_window_kernel(int vh, int pv, const char *ring, size_t vb, char *pw0,
+template <int KU>
+__global__ void __launch_bounds__(kBSm, 2) ms_window_kernel(int vh, int pv, const char *ring, size_t vb, char *pw0,
                                                          char *x0, MsState *st)
 {
     __shared__ double sc[kMaxShift], se[kMaxShift], sd[kMaxShift][kWin], sf[kMaxShift][kWin];
@@ -188,7 +189,7 @@ __global__ void __launch_bounds__(kBSm) ms_window_kernel(int vh, int pv, const c
     }
     __syncthreads();
     const int i = blockIdx.x * kBSm + threadIdx.x;
-    if (i < vh) window_update_site(ring, vb, pv, i, n, kmax, sc, se, sd, sf, pw0, x0);
+    if (i < vh) window_update_site<KU>(ring, vb, pv, i, n, kmax, sc, se, sd, sf, pw0, x0);
     // last block resets the window
     __shared__ bool last;
     __syncthreads();
@@ -203,6 +204,17 @@ __global__ void __launch_bounds__(kBSm) ms_window_kernel(int vh, int pv, const c
     }
 }
 
+// shifts updated per step of the window kernel's loop (KUQCD_WINDOW_UNROLL = 1 | 2 | 4)
+static int window_unroll()
+{
+    static const int k = [] {
+        const char *e = getenv("KUQCD_WINDOW_UNROLL");
+        const int v = e ? atoi(e) : 4;
+        return v == 1 || v == 2 ? v : 4;
+    }();
+    return k;
+}
+
 // ---------------------------------------------------------------------------------------------------- driver
 template <int LP, int SO>
 static void enqueue_ms_chunk(const Geom &g, const GaugeDev &gd, const MsBuffers &w, int parity, cudaStream_t s)
@@ -215,7 +227,11 @@ static void enqueue_ms_chunk(const Geom &g, const GaugeDev &gd, const MsBuffers 
                                                       w.vb, parity, w.st, w.partials);
         ms_p0_kernel<<<nb, kBSm, 0, s>>>(g.vh, pv, (const char *)w.ring, w.vb, w.p0, w.st);
     }
-    ms_window_kernel<<<nb, kBSm, 0, s>>>(g.vh, pv, (const char *)w.ring, w.vb, (char *)w.pw, (char *)w.x, w.st);
+    switch (window_unroll()) {
+        case 1: ms_window_kernel<1><<<nb, kBSm, 0, s>>>(g.vh, pv, (const char *)w.ring, w.vb, (char *)w.pw, (char *)w.x, w.st); break;
+        case 2: ms_window_kernel<2><<<nb, kBSm, 0, s>>>(g.vh, pv, (const char *)w.ring, w.vb, (char *)w.pw, (char *)w.x, w.st); break;
+        default: ms_window_kernel<4><<<nb, kBSm, 0, s>>>(g.vh, pv, (const char *)w.ring, w.vb, (char *)w.pw, (char *)w.x, w.st); break;
+    }
 }
 
 size_t ms_workspace_bytes(const Geom &g, int ns)
