@@ -17,6 +17,7 @@
 // window of the actual batch (kq_tune.cu), cached on disk.  Systems large enough to fill the GPU alone go through
 // the single-system solver instead, concurrently with the batched small ones (kq_batch_solve).
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cmath>
@@ -1429,6 +1430,14 @@ static int large_sites()
     return e ? atoi(e) : 131072;
 }
 
+// host threads solving the large systems at once (KUQCD_BATCH_LARGE_THREADS, 1 .. 8)
+static int large_threads()
+{
+    const char *e = getenv("KUQCD_BATCH_LARGE_THREADS");
+    const int v = e ? atoi(e) : 2;
+    return v >= 1 && v <= 8 ? v : 2;
+}
+
 KQ_API KuQCDStatus kq_batch_solve(kq_batch *b, kq_batch_info *out)
 {
     kq::NvtxRange nvtx_range_("kq_batch_solve");
@@ -1473,22 +1482,39 @@ KQ_API KuQCDStatus kq_batch_solve(kq_batch *b, kq_batch_info *out)
             st_small = solve_batched(b, &bi);
             if (st_small != KUQCD_SUCCESS) err_small = last_error();
         });
+    // The large systems, each on its own context's stream, on large_threads() host threads at once: one solve's
+    // latency-bound steps (reductions, scalar steps, the refinement's small grids) overlap another's kernels.
     KuQCDStatus st_large = KUQCD_SUCCESS;
+    std::string err_large;
     double worst = 0.0;
     int maxit = 0, refined = 0;
     long long launches = 0;
-    for (int i : large) {
-        BatchSystem &S = all[i];
-        kq_solve_param p = S.param;
-        p.shifts = S.shifts.data();
-        const KuQCDStatus st = kq_solve_multishift_device(S.ctx, &p, S.d_b, S.d_x, &S.info);
-        if (st != KUQCD_SUCCESS && st_large == KUQCD_SUCCESS) st_large = st;
-        maxit = std::max(maxit, S.info.iter);
-        launches += S.info.kernel_launches;
-        if (S.info.iter_refine > 0) ++refined;
-        if (S.param.solver == KQ_SOLVER_MIXED)
-            for (int k = 0; k < S.param.num_shift; ++k) worst = std::max(worst, S.info.true_residual[k]);
-    }
+    std::atomic<size_t> next_large{0};
+    std::mutex large_mu;
+    auto large_worker = [&]() {
+        cudaSetDevice(b->device);
+        for (size_t q; (q = next_large.fetch_add(1)) < large.size();) {
+            BatchSystem &S = all[large[q]];
+            kq_solve_param p = S.param;
+            p.shifts = S.shifts.data();
+            const KuQCDStatus st = kq_solve_multishift_device(S.ctx, &p, S.d_b, S.d_x, &S.info);
+            std::lock_guard<std::mutex> lk(large_mu);
+            if (st != KUQCD_SUCCESS && st_large == KUQCD_SUCCESS) {
+                st_large = st;
+                err_large = last_error();
+            }
+            maxit = std::max(maxit, S.info.iter);
+            launches += S.info.kernel_launches;
+            if (S.info.iter_refine > 0) ++refined;
+            if (S.param.solver == KQ_SOLVER_MIXED)
+                for (int k = 0; k < S.param.num_shift; ++k) worst = std::max(worst, S.info.true_residual[k]);
+        }
+    };
+    std::vector<std::thread> large_threads_v;
+    const int nlw = (int)std::min<size_t>((size_t)large_threads(), large.size());
+    for (int t = 1; t < nlw; ++t) large_threads_v.emplace_back(large_worker);
+    large_worker();
+    for (auto &t : large_threads_v) t.join();
     if (th.joinable()) th.join();
     for (size_t j = 0; j < small.size(); ++j) all[small[j]].info = b->sys[j].info;
     b->sys.swap(all);
@@ -1515,5 +1541,6 @@ KQ_API KuQCDStatus kq_batch_solve(kq_batch *b, kq_batch_info *out)
         set_last_error(err_small);
         return st_small;
     }
+    if (st_large != KUQCD_SUCCESS) set_last_error(err_large);
     return st_large;
 }

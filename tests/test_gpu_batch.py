@@ -97,13 +97,15 @@ def test_batch_argument_checks(cuda):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("large_sites", [256, 1])
-def test_batch_with_large_systems_on_the_single_system_solver(cuda, tmp_path, monkeypatch, large_sites):
-    """Systems of at least KUQCD_BATCH_LARGE_SITES sites per parity go through the single-system solver while the
-    rest are batched (256: two of each kind, overlapping on the GPU; 1: every system on its own); each system still
-    reaches its target and reports its own status and iterations."""
+@pytest.mark.parametrize("large_sites,threads", [(256, 2), (1, 1), (1, 3)])
+def test_batch_with_large_systems_on_the_single_system_solver(cuda, tmp_path, monkeypatch, large_sites, threads):
+    """Systems of at least KUQCD_BATCH_LARGE_SITES sites per parity go through the single-system solver, on
+    KUQCD_BATCH_LARGE_THREADS host threads at once, while the rest are batched (256: two of each kind, overlapping on
+    the GPU; 1: every system on its own); each system still reaches its target and reports its own status and
+    iterations."""
     monkeypatch.setenv("KUQCD_TUNE_CACHE", str(tmp_path / "tune.txt"))
     monkeypatch.setenv("KUQCD_BATCH_LARGE_SITES", str(large_sites))
+    monkeypatch.setenv("KUQCD_BATCH_LARGE_THREADS", str(threads))
     batch = K.Batch()
     keep = []
     for dims, eps, mass, ns, parity, seed in SYSTEMS:
