@@ -257,6 +257,8 @@ def exchange_link_ghosts(slabs, transport):
     torch.cuda.synchronize()
     # a link face travels up in t only: send it as the 'hi' face, receive it as the lower ghost
     ghosts = transport.exchange([(f, f) for f in faces])
+    # the received faces are ordered on torch's stream only, and kq_slab_set_link_ghosts copies on the context's
+    torch.cuda.synchronize()
     for s, (glo, _) in zip(slabs, ghosts):
         s.set_link_ghosts(glo)
 
